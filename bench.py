@@ -1,0 +1,313 @@
+"""Benchmark: runs/s of statistical model checking on the 100-agent SEIR
+epidemic network, Pr[<=100](<> R >= 50), 1,000,000 runs per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one pass of the hot path over one batch: 1e6 independent runs of
+the epidemic network (seeded synthetic input: the network comes from
+cusmc_b200.netgen.epidemic; every step uses a fresh stretch of the random
+stream).  `value` is whole-job runs/s with the network already resident on
+the device, timed with CUDA events on the launching stream around the
+simulation kernels; `e2e` is the same metric through the host-buffer C-ABI
+call csmc_run_host (network upload, simulation, per-run flag/value copies
+back to pageable host memory, all inside the timed region).  Under torchrun
+every rank simulates its own run range (weak scaling, no data-path
+collective); times are the max over ranks.
+
+--impl reference times the reference cuSMC binary, built from the reference
+sources for sm_100a by oracle/ref/Makefile (oracle/_ref/cusmc_ref_v8: limits
+raised to 8 variables / 8 enabled edges), on the same model file and query,
+from its own "Time taken" report (kernel + synchronise, smc.cu:234-255), on
+rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RUNS_PER_STEP = 1_000_000
+SEED = 20241203
+METRIC = "runs/s at 1 B200 (100-agent SEIR epidemic, Pr[<=100](<> R>=50))"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def epidemic_blob():
+    from cusmc_b200 import api, netgen
+    w = netgen.epidemic(n_agents=100, runs=RUNS_PER_STEP)
+    d = tempfile.mkdtemp(prefix="csmc_bench_")
+    path = w.write(os.path.join(d, "epidemic_100.xml"))
+    blob = api.compile_model(path)
+    q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, is_estimate=False)
+    return w, path, blob, q
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(blob, q, budget_s: float = 12.0):
+    """The CPU oracle on all host threads, on a bounded sample of the same
+    workload (runs from the same stream)."""
+    import oracle
+    threads = os.cpu_count() or 1
+    n = max(threads * 4, 64)
+    _, _, ms = oracle.run(blob, q, SEED, n, first_run=0, threads=threads)
+    rate = n / (ms / 1000.0)
+    n2 = int(min(max(rate * budget_s, n), 200_000))
+    r, _, ms2 = oracle.run(blob, q, SEED, n2, first_run=0, threads=threads)
+    return {"value": n2 / (ms2 / 1000.0), "unit": "runs/s", "cores": threads, "kind": "port",
+            "sample": f"{n2} runs of the same network and query (runs 0..{n2 - 1} of the stream), "
+                      f"{ms2 / 1000.0:.1f} s on {threads} host threads"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from cusmc_b200 import api
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    w, path, blob, q = epidemic_blob()
+    net = api.Network(blob)
+    n = RUNS_PER_STEP
+    dev = torch.device("cuda", local)
+    flags = torch.empty(n, dtype=torch.uint8, device=dev)
+    values = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def first_run_of(step):
+        return (step * world + rank) * n
+
+    for s in range(args.warmup):
+        net.run(q, SEED, n, first_run_of(1000 + s), flags=flags, values=values, stream=stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    kernel_ms = []
+    hits = 0
+    steps_total = 0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        ev[s][0].record()
+        r = net.run(q, SEED, n, first_run_of(s), flags=flags, values=values, stream=stream)
+        ev[s][1].record()
+        kernel_ms.append(r.kernel_ms)
+        hits += r.hits
+        steps_total += r.steps
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_total = sum(step_ms)
+    t_kernel = sum(kernel_ms)
+    if world > 1:
+        t = torch.tensor([t_total, t_kernel], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total, t_kernel = t.tolist()
+        c = torch.tensor([hits, steps_total], dtype=torch.int64, device=dev)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        hits, steps_total = c.tolist()
+    runs_total = n * args.steps * world
+    value = runs_total / (t_total / 1000.0)
+
+    # end to end through the host-buffer C-ABI call (rank-local)
+    e2e_ms = []
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        api.run_host(blob, q, SEED, n, first_run_of(2000 + s))
+        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+    e2e_t = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = t.item()
+    e2e_value = runs_total / (e2e_t / 1000.0)
+
+    peak, peak_kind = load_peaks()
+    # algorithmic HBM bytes of one simulation launch: the network staged once
+    # per CTA plus one flag byte and one 8-byte value per run
+    plan = net.plan()
+    lanes, cpl, rpc = plan
+    ctas = min((n + rpc - 1) // rpc, 148 * 8)
+    alg_bytes = len(blob) * ctas + 9 * n
+    achieved = alg_bytes / (t_kernel / args.steps / 1000.0) / 1e9
+    comp_steps = steps_total / world * 100 / args.steps  # component-steps per launch on this rank
+    line = {
+        "metric": METRIC, "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 state / f64 expressions", "data": "synthetic (seeded generated network)",
+        "config": {"workload": "epidemic_100 (SEIR, 100 agents, beta=0.3, E->I 0.2, I->R 0.1), T=100, "
+                               "Pr[<=100](<> R>=50), 1e6 runs per step per GPU",
+                   "runs_per_step_per_gpu": n, "lanes_per_run": lanes, "comps_per_lane": cpl,
+                   "runs_per_cta": rpc, "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"runs sharded over {world} GPU(s)"},
+        "estimate": hits / runs_total,
+        "race_steps_per_run": steps_total / runs_total,
+        "component_steps_per_s": steps_total * 100 / (t_total / 1000.0),
+        "e2e": {"value": e2e_value, "unit": "runs/s", "h2d_bytes_per_step": len(blob),
+                "d2h_bytes_per_step": 9 * n},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "note": "issue-bound kernel: HBM bytes per launch are the staged network and 9 B/run "
+                             "of results; see issue figures from ncu in profiles/"},
+        "clocks": clocks,
+        "gpu_launches": 2 * args.steps,
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(blob, q)
+    net.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    binary = os.path.join(ROOT, "oracle", "_ref", "cusmc_ref_v8")
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cusmc_ref_v8 was not built "
+                          "(the reference checkout is needed at build time)"}))
+        return
+    w, path, blob, q = epidemic_blob()
+    work = tempfile.mkdtemp(prefix="csmc_ref_")
+    cwd = os.path.join(work, "run")  # the reference writes ../results5.csv
+    os.makedirs(cwd)
+
+    def once(runs, seed):
+        cmd = [binary, "-m", path, "-s", str(seed), "-q", str(runs), str(w.horizon), str(w.threshold),
+               str(w.var_id), "1", "0", ""]
+        out = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
+        ms = None
+        result = None
+        for line in out.stdout.splitlines():
+            if line.startswith("Time taken:") and line.endswith(path) and " ms on file " in line:
+                ms = float(line.split()[2])
+            if line.startswith("Result:"):
+                result = float(line.split()[1])
+        if ms is None:
+            raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
+        return ms, result
+
+    probe_ms, _ = once(20_000, 1)
+    rate = 20_000 / (probe_ms / 1000.0)
+    sample = int(min(RUNS_PER_STEP, max(20_000, rate * 10.0)))
+    for s in range(args.warmup):
+        once(sample, 100 + s)
+    times, results = [], []
+    for s in range(args.steps):
+        ms, res = once(sample, 1 + s)
+        times.append(ms)
+        results.append(res)
+    value = sample * args.steps / (sum(times) / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum(times) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 state / f64 expressions",
+        "data": "synthetic (seeded generated network)", "impl": "reference",
+        "config": {"workload": "epidemic_100 (SEIR, 100 agents), T=100, Pr[<=100](<> R>=50)",
+                   "runs_per_step": sample, "binary": "reference cuSMC built for sm_100a, MAX_VARIABLES=8, "
+                                                     "MAX_EDGES_PER_NODE=8"},
+        "estimate": statistics.mean(results) if results else None,
+        "cpu_baseline": {"value": value, "unit": "runs/s", "cores": 1, "kind": "reference",
+                         "sample": f"{sample} runs per step; the reference's simulation path is its GPU kernel "
+                                   "(it has no CPU implementation)"},
+        "e2e": {"value": value, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

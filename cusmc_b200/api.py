@@ -1,0 +1,195 @@
+"""Host-side interface over the C ABI, mirroring the reference's operator
+interface for the simulation path.
+
+Reference interface (AndreasHolt/cuSMC) and its counterpart here:
+
+* ``smc(configuration, statistics_Configuration)`` (smc.cuh:14, smc.cu:283)
+  -> :func:`smc` with :class:`Configuration` / :class:`StatisticsConfiguration`
+  (same fields as main.cuh:33-58); prints the same report.
+* ``init_shared_model_state(...)`` (simulation/state/shared_model_state.cuh:219)
+  -> :func:`compile_model` + :class:`Network` (upload of the packed network).
+* ``run_statistical_model_checking(...)`` (smc.cu:11) plus ``Statistics``
+  collection (simulation/statistics.cuh:126-163) -> :meth:`Network.run`
+  (device outputs) and :func:`run_host` (host outputs, copies included).
+
+Per-run device buffers are torch CUDA tensors (torch is used for device
+memory and streams only); every simulation runs in the sm_100a kernels of
+libcsmc.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from ._native import QUERY_LOCATION, QUERY_VARIABLE, Query, Result, check, lib
+
+
+@dataclass
+class Configuration:
+    """main.cuh:33-36."""
+
+    filename: str
+    curand_seed: int = 1235
+
+
+@dataclass
+class StatisticsConfiguration:
+    """main.cuh:46-58 (``statistics_Configuration``)."""
+
+    simulations: int = 16384
+    timeBound: int = 100
+    variable_threshhold: int = -1
+    variable_id: int = 1
+    isMax: bool = True
+    isEstimate: bool = True
+    loc_query: str = ""
+
+
+def make_query(kind: int = QUERY_VARIABLE, var_id: int = -1, is_max: bool = True, is_estimate: bool = False,
+               threshold: float = 0.0, horizon: float = 100.0, max_steps: int = 0) -> Query:
+    q = Query()
+    q.kind = kind
+    q.var_id = var_id
+    q.is_max = 1 if is_max else 0
+    q.is_estimate = 1 if is_estimate else 0
+    q.threshold = float(threshold)
+    q.horizon = float(horizon)
+    q.max_steps = int(max_steps)
+    return q
+
+
+def location_query(horizon: float, max_steps: int = 0) -> Query:
+    return make_query(QUERY_LOCATION, -1, True, False, 0.0, horizon, max_steps)
+
+
+def variable_query(var_id: int, horizon: float, threshold: float = 0.0, is_max: bool = True,
+                   is_estimate: bool = False, max_steps: int = 0) -> Query:
+    return make_query(QUERY_VARIABLE, var_id, is_max, is_estimate, threshold, horizon, max_steps)
+
+
+def compile_model(path: str, loc_query: str = "", loc_mode: bool = False) -> bytes:
+    """Parses a UPPAAL model with the reference's front-end semantics and
+    returns the packed network blob."""
+    blob = ctypes.c_void_p()
+    size = ctypes.c_size_t()
+    check(lib().csmc_model_compile(path.encode(), loc_query.encode(), 1 if loc_mode else 0,
+                                   ctypes.byref(blob), ctypes.byref(size)))
+    try:
+        return ctypes.string_at(blob, size.value)
+    finally:
+        lib().csmc_free(blob)
+
+
+def dump_model(path: str, loc_query: str = "", loc_mode: bool = False) -> str:
+    """Canonical text form of the network as the kernel receives it."""
+    text = ctypes.c_void_p()
+    check(lib().csmc_model_dump(path.encode(), loc_query.encode(), 1 if loc_mode else 0, ctypes.byref(text)))
+    try:
+        return ctypes.string_at(text).decode()
+    finally:
+        lib().csmc_free(text)
+
+
+def blob_info(blob: bytes) -> dict:
+    nv, nc, nl = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    check(lib().csmc_blob_info(blob, len(blob), ctypes.byref(nv), ctypes.byref(nc), ctypes.byref(nl)))
+    return {"n_vars": nv.value, "n_comps": nc.value, "n_locs": nl.value}
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+class Network:
+    """A packed network resident on the current CUDA device."""
+
+    def __init__(self, blob: bytes):
+        self.blob = blob
+        self.info = blob_info(blob)
+        h = ctypes.c_void_p()
+        check(lib().csmc_net_upload(blob, len(blob), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            lib().csmc_net_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def plan(self) -> tuple[int, int, int]:
+        a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(lib().csmc_plan(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def run(self, query: Query, seed: int, n_runs: int, first_run: int = 0, flags=None, values=None, steps=None,
+            stream: int | None = None) -> Result:
+        """Simulates runs on the device; flags/values/steps are optional torch
+        CUDA tensors (uint8 / float64 / int32) of at least n_runs entries."""
+        r = Result()
+        check(lib().csmc_run(self._h, ctypes.byref(query), seed & (2**64 - 1), first_run, n_runs, _ptr(flags),
+                             _ptr(values), _ptr(steps), ctypes.byref(r), stream))
+        return r
+
+    def run_verify(self, query: Query, seed: int, n_runs: int, first_run: int = 0):
+        """Runs the verification variant; returns (Result, dict of numpy arrays)."""
+        import torch
+        dev = torch.device("cuda")
+        C, V = self.info["n_comps"], self.info["n_vars"]
+        flags = torch.zeros(n_runs, dtype=torch.uint8, device=dev)
+        values = torch.zeros(n_runs, dtype=torch.float64, device=dev)
+        steps = torch.zeros(n_runs, dtype=torch.int32, device=dev)
+        digests = torch.zeros(n_runs, dtype=torch.int64, device=dev)
+        final = torch.zeros(n_runs * (C + V), dtype=torch.int32, device=dev)
+        r = Result()
+        check(lib().csmc_run_verify(self._h, ctypes.byref(query), seed & (2**64 - 1), first_run, n_runs,
+                                    _ptr(flags), _ptr(values), _ptr(steps), _ptr(digests), _ptr(final),
+                                    ctypes.byref(r), None))
+        out = {
+            "flags": flags.cpu().numpy(),
+            "values": values.cpu().numpy(),
+            "steps": steps.cpu().numpy().view(np.uint32),
+            "digests": digests.cpu().numpy().view(np.uint64),
+            "final_state": final.cpu().numpy().view(np.uint32).reshape(n_runs, C + V),
+        }
+        return r, out
+
+
+def run_host(blob: bytes, query: Query, seed: int, n_runs: int, first_run: int = 0, want_steps: bool = False):
+    """Host buffers in and out (upload, kernel, copies back). Returns
+    (Result, flags, values, steps-or-None) with numpy arrays."""
+    flags = np.zeros(n_runs, dtype=np.uint8)
+    values = np.zeros(n_runs, dtype=np.float64)
+    steps = np.zeros(n_runs, dtype=np.uint32) if want_steps else None
+    r = Result()
+    check(lib().csmc_run_host(blob, len(blob), ctypes.byref(query), seed & (2**64 - 1), first_run, n_runs,
+                              flags.ctypes.data, values.ctypes.data,
+                              None if steps is None else steps.ctypes.data, ctypes.byref(r)))
+    return r, flags, values, steps
+
+
+def smc(conf: Configuration, stat_conf: StatisticsConfiguration) -> None:
+    """The reference's ``smc()``: parse, simulate, print the report, update
+    ../results5.csv."""
+    check(lib().csmc_smc(conf.filename.encode(), int(conf.curand_seed), int(stat_conf.simulations),
+                         int(stat_conf.timeBound), int(stat_conf.variable_threshhold), int(stat_conf.variable_id),
+                         1 if stat_conf.isMax else 0, 1 if stat_conf.isEstimate else 0,
+                         stat_conf.loc_query.encode()))
+
+
+def version() -> str:
+    return lib().csmc_version().decode()
+
+
+__all__ = [
+    "Configuration", "StatisticsConfiguration", "Network", "Query", "Result", "compile_model", "dump_model",
+    "blob_info", "make_query", "location_query", "variable_query", "run_host", "smc", "version",
+    "QUERY_LOCATION", "QUERY_VARIABLE", "_native",
+]

@@ -1,0 +1,505 @@
+// C ABI of libcsmc (include/csmc.h): front end, device network handles,
+// launches, result collection, and the reference's smc() report.
+#include "../../include/csmc.h"
+#include "front/front.h"
+#include "include/csmc_net.h"
+#include "include/csmc_numeric.h"
+#include "kernels/sim.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+struct csmc_net {
+    int device = 0;
+    uint8_t *d_blob = nullptr;
+    uint32_t bytes = 0;       // staged bytes (multiple of 16)
+    csmc_net_header h{};
+    unsigned long long *d_scratch = nullptr;
+    // internal per-run buffers used when the caller passes none
+    uint8_t *d_flags = nullptr;
+    double *d_values = nullptr;
+    uint64_t cap_runs = 0;
+    double *d_partials = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int lanes = 0, comps_per_lane = 0, block = 256, grid = 0;
+    size_t smem = 0;
+    uint32_t state_stride = 0;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &m) {
+    g_err = m;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(CSMC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(x, what)                          \
+    do {                                     \
+        cudaError_t e_ = (x);                \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// Lane-group shape for C components: one lane per component up to a warp,
+// then a full warp with K components per lane.
+void choose_shape(uint32_t C, int &G, int &K) {
+    if (C <= 32) {
+        G = 1;
+        while (static_cast<uint32_t>(G) < C) G <<= 1;
+        K = 1;
+        return;
+    }
+    G = 32;
+    K = 2;
+    while (static_cast<uint32_t>(G * K) < C) K <<= 1;
+}
+
+const csmc_net_header *header_of(const void *blob, size_t bytes) {
+    if (!blob || bytes < sizeof(csmc_net_header)) return nullptr;
+    const auto *h = static_cast<const csmc_net_header *>(blob);
+    if (h->magic != CSMC_NET_MAGIC || h->version != CSMC_NET_VERSION || h->total_bytes > bytes) return nullptr;
+    return h;
+}
+
+int ensure_buffers(csmc_net *n, uint64_t runs) {
+    if (runs <= n->cap_runs) return CSMC_OK;
+    cudaFree(n->d_flags);
+    cudaFree(n->d_values);
+    n->d_flags = nullptr;
+    n->d_values = nullptr;
+    n->cap_runs = 0;
+    CK(cudaMalloc(&n->d_flags, runs), "cudaMalloc(flags)");
+    CK(cudaMalloc(&n->d_values, runs * sizeof(double)), "cudaMalloc(values)");
+    n->cap_runs = runs;
+    return CSMC_OK;
+}
+
+// Deterministic sum and sum of squares of values[0..n): fixed chunking,
+// fixed per-thread order and a fixed shared-memory tree.
+constexpr int kReduceBlocks = 256;
+__global__ void reduce_values(const double *values, uint64_t n, double *partials) {
+    __shared__ double s1[256], s2[256];
+    const uint64_t chunk = (n + kReduceBlocks - 1) / kReduceBlocks;
+    const uint64_t b0 = blockIdx.x * chunk, b1 = (b0 + chunk < n) ? b0 + chunk : n;
+    double a = 0.0, q = 0.0;
+    for (uint64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const double v = values[i];
+        a = csmc::d_add(a, v);
+        q = csmc::d_add(q, csmc::d_mul(v, v));
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = q;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s1[threadIdx.x] = csmc::d_add(s1[threadIdx.x], s1[threadIdx.x + s]);
+            s2[threadIdx.x] = csmc::d_add(s2[threadIdx.x], s2[threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = s1[0];
+        partials[2 * blockIdx.x + 1] = s2[0];
+    }
+}
+
+int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t first_run, uint64_t n_runs,
+             uint8_t *flags, double *values, uint32_t *steps, uint64_t *digests, uint32_t *final_state,
+             csmc_result *out, void *stream, bool verify) {
+    if (!cn || !q || !out) return fail(CSMC_ERR_ARG, "null argument");
+    csmc_net *n = const_cast<csmc_net *>(cn);
+    if (q->kind != CSMC_QUERY_LOCATION && q->kind != CSMC_QUERY_VARIABLE) return fail(CSMC_ERR_ARG, "bad query kind");
+    if (q->kind == CSMC_QUERY_VARIABLE && (q->var_id < 0 || static_cast<uint32_t>(q->var_id) >= n->h.n_vars))
+        return fail(CSMC_ERR_ARG, "query variable id " + std::to_string(q->var_id) + " out of range");
+    if (first_run + n_runs < first_run || first_run + n_runs > (1ull << 62))
+        return fail(CSMC_ERR_ARG, "run range out of bounds");
+    std::memset(out, 0, sizeof *out);
+    out->runs = n_runs;
+    out->lanes_per_run = n->lanes;
+    out->comps_per_lane = n->comps_per_lane;
+    out->runs_per_cta = n->block / n->lanes;
+    if (n_runs == 0) return CSMC_OK;
+    CK(cudaSetDevice(n->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool need_values = q->kind == CSMC_QUERY_VARIABLE;
+    if (need_values && !values) {
+        int rc = ensure_buffers(n, n_runs);
+        if (rc) return rc;
+        values = n->d_values;
+    }
+    CK(cudaMemsetAsync(n->d_scratch, 0, CSMC_SCRATCH_WORDS * sizeof(unsigned long long), st), "cudaMemsetAsync");
+    csmc::SimParams p{};
+    p.blob = n->d_blob;
+    p.blob_bytes = n->bytes;
+    p.state_stride = n->state_stride;
+    p.loc_mode = q->kind == CSMC_QUERY_LOCATION;
+    p.var_id = q->var_id;
+    p.is_max = q->is_max;
+    p.threshold = q->threshold;
+    p.horizon = static_cast<float>(q->horizon);
+    p.max_steps = q->max_steps ? q->max_steps : 10000000ull;
+    p.seed = seed;
+    p.first_run = first_run;
+    p.n_runs = n_runs;
+    p.flags = flags;
+    p.values = values;
+    p.steps = steps;
+    p.digests = digests;
+    p.final_state = final_state;
+    p.scratch = n->d_scratch;
+    int ctas = 0;
+    int rc = csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas);
+    if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
+    if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network (shared memory)");
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device), "cudaDeviceGetAttribute");
+    const uint64_t groups_per_cta = static_cast<uint64_t>(n->block / n->lanes);
+    uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(ctas);
+    const uint64_t needed = (n_runs + groups_per_cta - 1) / groups_per_cta;
+    if (grid > needed) grid = needed;
+    n->grid = static_cast<int>(grid);
+    CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
+    rc = csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block, n->smem, st);
+    if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
+    CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
+    if (need_values) reduce_values<<<kReduceBlocks, 256, 0, st>>>(values, n_runs, n->d_partials);
+    unsigned long long sc[CSMC_SCRATCH_WORDS];
+    CK(cudaMemcpyAsync(sc, n->d_scratch, sizeof sc, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(scratch)");
+    std::vector<double> part(2 * kReduceBlocks, 0.0);
+    if (need_values)
+        CK(cudaMemcpyAsync(part.data(), n->d_partials, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
+           "cudaMemcpyAsync(partials)");
+    CK(cudaStreamSynchronize(st), "simulation kernel");
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, n->ev0, n->ev1), "cudaEventElapsedTime");
+    out->kernel_ms = ms;
+    out->hits = sc[1];
+    out->steps = sc[2];
+    out->capped = sc[3];
+    for (int b = 0; b < kReduceBlocks; ++b) {
+        out->sum += part[2 * b];
+        out->sum_sq += part[2 * b + 1];
+    }
+    if (q->kind == CSMC_QUERY_VARIABLE && q->is_estimate) out->estimate = out->sum / static_cast<double>(n_runs);
+    else out->estimate = static_cast<double>(out->hits) / static_cast<double>(n_runs);
+    return CSMC_OK;
+}
+
+// writeTimingToCSV of the reference (simulation/write_csv.cu:15-98): one row
+// per model file name, one column per "MC<n>_Sim<n>_Time<T>" configuration,
+// ';'-separated, at <parent of cwd>/results5.csv.
+void write_timing_csv(const std::string &xml_path, int mc, int sims, double time_bound, double ms) {
+    namespace fs = std::filesystem;
+    const fs::path csv = fs::current_path().parent_path() / "results5.csv";
+    const std::string fname = fs::path(xml_path).filename().string();
+    std::ostringstream ts;
+    ts << std::fixed << std::setprecision(2) << time_bound;
+    const std::string config = "MC" + std::to_string(mc) + "_Sim" + std::to_string(sims) + "_Time" + ts.str();
+    std::vector<std::vector<std::string>> rows;
+    if (fs::exists(csv)) {
+        std::ifstream f(csv);
+        std::string line;
+        while (std::getline(f, line)) {
+            std::vector<std::string> row;
+            std::stringstream ls(line);
+            std::string cell;
+            while (std::getline(ls, cell, ';')) row.push_back(cell);
+            rows.push_back(row);
+        }
+    }
+    if (rows.empty()) rows.push_back({""});
+    size_t col = 0;
+    for (size_t c = 1; c < rows[0].size(); ++c)
+        if (rows[0][c] == config) { col = c; break; }
+    if (!col) {
+        col = rows[0].size();
+        rows[0].push_back(config);
+    }
+    size_t row = 0;
+    for (size_t r = 1; r < rows.size(); ++r)
+        if (!rows[r].empty() && rows[r][0] == fname) { row = r; break; }
+    if (!row) {
+        row = rows.size();
+        rows.push_back({fname});
+    }
+    for (auto &r : rows)
+        while (r.size() <= col) r.push_back("");
+    rows[row][col] = std::to_string(ms);
+    std::ofstream o(csv);
+    if (!o.is_open()) {
+        std::cerr << "Failed to open file for writing" << std::endl;
+        return;
+    }
+    for (const auto &r : rows) {
+        o << r[0];
+        for (size_t i = 1; i < r.size(); ++i) o << ";" << r[i];
+        o << "\n";
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *csmc_last_error(void) { return g_err.c_str(); }
+
+const char *csmc_version(void) { return "csmc-b200 0.1 (sm_100a)"; }
+
+void csmc_free(void *p) { std::free(p); }
+
+int csmc_model_compile(const char *xml_path, const char *loc_query, int loc_mode, void **blob, size_t *bytes) {
+    if (!xml_path || !blob || !bytes) return fail(CSMC_ERR_ARG, "null argument");
+    try {
+        auto net = csmc::parse_uppaal_file(xml_path);
+        csmc::DevModel m = csmc::build_device_model(*net, loc_query ? loc_query : "", loc_mode != 0);
+        std::vector<uint8_t> b = csmc::pack_device_model(m);
+        void *p = std::malloc(b.size());
+        if (!p) return fail(CSMC_ERR_ARG, "out of host memory");
+        std::memcpy(p, b.data(), b.size());
+        *blob = p;
+        *bytes = b.size();
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_MODEL, e.what());
+    }
+}
+
+int csmc_model_dump(const char *xml_path, const char *loc_query, int loc_mode, char **text) {
+    if (!xml_path || !text) return fail(CSMC_ERR_ARG, "null argument");
+    try {
+        auto net = csmc::parse_uppaal_file(xml_path);
+        csmc::DevModel m = csmc::build_device_model(*net, loc_query ? loc_query : "", loc_mode != 0);
+        const std::string s = csmc::dump_device_model(m);
+        char *p = static_cast<char *>(std::malloc(s.size() + 1));
+        std::memcpy(p, s.c_str(), s.size() + 1);
+        *text = p;
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_MODEL, e.what());
+    }
+}
+
+int csmc_blob_info(const void *blob, size_t bytes, uint32_t *n_vars, uint32_t *n_comps, uint32_t *n_locs) {
+    const csmc_net_header *h = header_of(blob, bytes);
+    if (!h) return fail(CSMC_ERR_ARG, "not a network blob");
+    if (n_vars) *n_vars = h->n_vars;
+    if (n_comps) *n_comps = h->n_comps;
+    if (n_locs) *n_locs = h->n_locs;
+    return CSMC_OK;
+}
+
+int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
+    if (!out) return fail(CSMC_ERR_ARG, "null argument");
+    *out = nullptr;
+    const csmc_net_header *h = header_of(blob, bytes);
+    if (!h) return fail(CSMC_ERR_ARG, "not a network blob");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(CSMC_ERR_NODEVICE, "no CUDA device is available (there is no CPU fallback)");
+    }
+    auto n = std::make_unique<csmc_net>();
+    CK(cudaGetDevice(&n->device), "cudaGetDevice");
+    n->h = *h;
+    n->bytes = (h->total_bytes + 15u) & ~15u;
+    choose_shape(h->n_comps, n->lanes, n->comps_per_lane);
+    if (!csmc::sim_supported(n->lanes, n->comps_per_lane))
+        return fail(CSMC_ERR_LIMIT, "networks with more than 1024 components are not supported");
+    n->state_stride = static_cast<uint32_t>((48 + 4 * h->n_vars + 15) & ~15u);
+    n->smem = n->bytes + static_cast<size_t>(n->block / n->lanes) * n->state_stride;
+    int max_smem = 0;
+    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device), "attribute");
+    if (n->smem > static_cast<size_t>(max_smem))
+        return fail(CSMC_ERR_LIMIT, "network (" + std::to_string(n->bytes) + " bytes) does not fit in shared memory");
+    CK(cudaMalloc(&n->d_blob, n->bytes), "cudaMalloc(network)");
+    CK(cudaMemset(n->d_blob, 0, n->bytes), "cudaMemset");
+    CK(cudaMemcpy(n->d_blob, blob, h->total_bytes, cudaMemcpyHostToDevice), "cudaMemcpy(network)");
+    CK(cudaMalloc(&n->d_scratch, CSMC_SCRATCH_WORDS * sizeof(unsigned long long)), "cudaMalloc(scratch)");
+    CK(cudaMalloc(&n->d_partials, 2 * kReduceBlocks * sizeof(double)), "cudaMalloc(partials)");
+    CK(cudaEventCreate(&n->ev0), "cudaEventCreate");
+    CK(cudaEventCreate(&n->ev1), "cudaEventCreate");
+    *out = n.release();
+    return CSMC_OK;
+}
+
+void csmc_net_free(csmc_net *n) {
+    if (!n) return;
+    cudaFree(n->d_blob);
+    cudaFree(n->d_scratch);
+    cudaFree(n->d_flags);
+    cudaFree(n->d_values);
+    cudaFree(n->d_partials);
+    if (n->ev0) cudaEventDestroy(n->ev0);
+    if (n->ev1) cudaEventDestroy(n->ev1);
+    delete n;
+}
+
+int csmc_plan(const csmc_net *n, int32_t *lanes, int32_t *cpl, int32_t *rpc) {
+    if (!n) return fail(CSMC_ERR_ARG, "null argument");
+    if (lanes) *lanes = n->lanes;
+    if (cpl) *cpl = n->comps_per_lane;
+    if (rpc) *rpc = n->block / n->lanes;
+    return CSMC_OK;
+}
+
+int csmc_run(const csmc_net *net, const csmc_query *q, uint64_t seed, uint64_t first_run, uint64_t n_runs,
+             uint8_t *flags, double *values, uint32_t *steps, csmc_result *out, void *stream) {
+    try {
+        return run_impl(net, q, seed, first_run, n_runs, flags, values, steps, nullptr, nullptr, out, stream, false);
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_ARG, e.what());
+    }
+}
+
+int csmc_run_verify(const csmc_net *net, const csmc_query *q, uint64_t seed, uint64_t first_run, uint64_t n_runs,
+                    uint8_t *flags, double *values, uint32_t *steps, uint64_t *digests, uint32_t *final_state,
+                    csmc_result *out, void *stream) {
+    try {
+        return run_impl(net, q, seed, first_run, n_runs, flags, values, steps, digests, final_state, out, stream,
+                        true);
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_ARG, e.what());
+    }
+}
+
+int csmc_run_host(const void *blob, size_t bytes, const csmc_query *q, uint64_t seed, uint64_t first_run,
+                  uint64_t n_runs, uint8_t *flags, double *values, uint32_t *steps, csmc_result *out) {
+    csmc_net *n = nullptr;
+    int rc = csmc_net_upload(blob, bytes, &n);
+    if (rc) return rc;
+    uint8_t *d_flags = nullptr;
+    double *d_values = nullptr;
+    uint32_t *d_steps = nullptr;
+    auto cleanup = [&] {
+        cudaFree(d_flags);
+        cudaFree(d_values);
+        cudaFree(d_steps);
+        csmc_net_free(n);
+    };
+    if (n_runs) {
+        if (cudaMalloc(&d_flags, n_runs) != cudaSuccess || cudaMalloc(&d_values, n_runs * sizeof(double)) != cudaSuccess ||
+            (steps && cudaMalloc(&d_steps, n_runs * sizeof(uint32_t)) != cudaSuccess)) {
+            cleanup();
+            return fail(CSMC_ERR_CUDA, "cudaMalloc(per-run outputs)");
+        }
+    }
+    rc = csmc_run(n, q, seed, first_run, n_runs, d_flags, d_values, d_steps, out, nullptr);
+    if (rc == CSMC_OK && n_runs) {
+        std::vector<double> v(values ? 0 : n_runs);
+        double *hv = values ? values : v.data();
+        cudaError_t e = cudaMemcpy(hv, d_values, n_runs * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && flags) e = cudaMemcpy(flags, d_flags, n_runs, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && steps) e = cudaMemcpy(steps, d_steps, n_runs * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(per-run outputs)");
+        else {
+            // the reference's host reduction order (smc.cu:378-402)
+            double s = 0.0, s2 = 0.0;
+            for (uint64_t i = 0; i < n_runs; ++i) {
+                s += hv[i];
+                s2 += hv[i] * hv[i];
+            }
+            out->sum = s;
+            out->sum_sq = s2;
+            if (q->kind == CSMC_QUERY_VARIABLE && q->is_estimate) out->estimate = s / static_cast<double>(n_runs);
+        }
+    }
+    cleanup();
+    return rc;
+}
+
+int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int threshold, int var_id, int is_max,
+             int is_estimate, const char *loc_query) {
+    if (!model_path) return fail(CSMC_ERR_ARG, "null model path");
+    const std::string lq = loc_query ? loc_query : "";
+    const bool loc_mode = var_id == -1;
+    void *blob = nullptr;
+    size_t bytes = 0;
+    int rc = csmc_model_compile(model_path, lq.c_str(), loc_mode ? 1 : 0, &blob, &bytes);
+    if (rc) return rc;
+    const csmc_net_header *h = header_of(blob, bytes);
+    std::printf("Set number of variables to: %d\n", static_cast<int>(h->n_vars));
+    std::fflush(stdout);
+    const int mc = static_cast<int>(h->n_comps);
+    std::cout << "=================\n\n";
+    std::cout << "Running SMC with the following settings:" << std::endl;
+    std::cout << "- Number of simulations: " << sims << std::endl;
+    std::cout << "- Model: " << model_path << std::endl;
+    std::cout << "- Random seed: " << seed << std::endl;
+    std::cout << "- Time bound: " << time_bound << std::endl;
+    std::cout << "- Num components: " << mc << std::endl;
+    if (!loc_mode)
+        std::cout << "- Logging type: variable query. Finding " << (is_max ? "max" : "min")
+                  << " of variable with ID " << var_id << std::endl;
+    else
+        std::cout << "- Logging type: location query on query: " << lq << std::endl;
+    std::cout << "=================\n\n";
+
+    csmc_query q{};
+    q.kind = loc_mode ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
+    q.var_id = var_id;
+    q.is_max = is_max;
+    q.is_estimate = is_estimate;
+    q.threshold = threshold;
+    q.horizon = static_cast<double>(static_cast<float>(time_bound));
+    const uint64_t n_runs = sims > 0 ? static_cast<uint64_t>(sims) : 0;
+    std::vector<uint8_t> flags(n_runs);
+    std::vector<double> values(n_runs);
+    csmc_result res{};
+    const auto t0 = std::chrono::steady_clock::now();
+    rc = csmc_run_host(blob, bytes, &q, static_cast<uint64_t>(static_cast<int64_t>(seed)), 0, n_runs, flags.data(),
+                       values.data(), nullptr, &res);
+    const auto dur = std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0);
+    std::free(blob);
+    if (rc) {
+        std::cout << "Error: " << g_err << std::endl;
+        return rc;
+    }
+    const double ms = dur.count() / 1000000.0;
+    std::cout << "Time taken: " << ms << " ms on file " << model_path << std::endl;
+    std::cout << "Time taken: " << dur.count() << " on file " << model_path << std::endl;
+    std::cout << "Time taken: " << dur.count() << " ns (" << (dur.count() / 1000000.0) << " ms)" << std::endl;
+    write_timing_csv(model_path, mc, sims, time_bound, ms);
+    if (!loc_mode) {
+        double result = 0;
+        if (is_estimate) {
+            for (uint64_t i = 0; i < n_runs; ++i) result += values[i];
+            result = result / static_cast<double>(sims);
+        } else {
+            for (uint64_t i = 0; i < n_runs; ++i) {
+                if (is_max && values[i] > threshold) result += 1;
+                if (!is_max && values[i] < threshold) result += 1;
+            }
+            result = result / static_cast<double>(sims);
+        }
+        std::cout << "Result: " << result << std::endl;
+    } else {
+        int hits = 0;
+        for (uint64_t i = 0; i < n_runs; ++i)
+            if (flags[i]) ++hits;
+        std::cout << "Number of simulations: " << n_runs << std::endl;
+        std::cout << "Number of hits: " << hits << std::endl;
+        std::cout << "The answer to " << lq << " is "
+                  << static_cast<float>(hits) / static_cast<float>(sims) << std::endl;
+    }
+    return CSMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// cusmc: drop-in command line for the reference cuSMC binary.
+//
+// Same grammar, defaults, messages and exit codes as the reference's main()
+// and HandleCommandLineArguments (main.cu:10-110):
+//   -m|--model PATH   -s|--seed INT
+//   -q|--query SIMS T THRESHOLD VAR_ID IS_MAX IS_ESTIMATE LOC_QUERY
+//   -h|--help
+// Exit code 1 after a simulation, 0 after -h or a command-line error.
+// Options of this build that the reference does not have use the --csmc-
+// prefix so the reference grammar stays intact.
+#include "../../../include/csmc.h"
+
+#include <iostream>
+#include <stdexcept>
+#include <string>
+
+namespace {
+
+struct StatConfig {  // statistics_Configuration, main.cuh:46-58
+    int simulations = 16384;
+    int time_bound = 100;
+    int threshold = -1;
+    int var_id = 1;
+    bool is_max = true;
+    bool is_estimate = true;
+    std::string loc_query;
+};
+
+bool handle_args(int argc, char **argv, std::string *filename, int *seed, StatConfig *stats) {
+    for (int i = 1; i < argc; i++) {
+        std::string arg = argv[i];
+        if (arg == "-m" || arg == "--model") {
+            if (i + 1 < argc) {
+                *filename = argv[++i];
+            } else {
+                std::cerr << "Error: -i option requires a value" << std::endl;
+                return false;
+            }
+        } else if (arg == "-s" || arg == "--seed") {
+            if (i + 1 < argc) {
+                const std::string str = argv[++i];
+                try {
+                    *seed = std::stoi(str);
+                } catch (const std::invalid_argument &e) {
+                    std::cerr << "Error: invalid argument: " << e.what() << std::endl;
+                    return false;
+                } catch (const std::out_of_range &e) {
+                    std::cerr << "Error: number too big: " << e.what() << std::endl;
+                    return false;
+                }
+            } else {
+                std::cerr << "Error: -s option requires a value" << std::endl;
+                return false;
+            }
+        } else if (arg == "-q" || arg == "--query") {
+            if (i + 7 < argc) {
+                const std::string sims = argv[++i], tb = argv[++i], thr = argv[++i], vid = argv[++i],
+                                  mx = argv[++i], est = argv[++i];
+                stats->loc_query = argv[++i];
+                try {
+                    stats->simulations = std::stoi(sims);
+                    stats->time_bound = std::stoi(tb);
+                    stats->threshold = std::stoi(thr);
+                    stats->var_id = std::stoi(vid);
+                    stats->is_max = static_cast<bool>(std::stoi(mx));
+                    stats->is_estimate = static_cast<bool>(std::stoi(est));
+                } catch (const std::invalid_argument &e) {
+                    std::cerr << "Error: invalid argument: " << e.what() << std::endl;
+                    return false;
+                } catch (const std::out_of_range &e) {
+                    std::cerr << "Error: number too big: " << e.what() << std::endl;
+                    return false;
+                }
+            } else {
+                std::cerr << "Error: -r option requires a value" << std::endl;
+                return false;
+            }
+        } else if (arg == "-h" || arg == "--help") {
+            std::cout << "Use -m or --model, followed by a path, for inputting a path the the model XML file."
+                      << std::endl;
+            std::cout << "Use -s or --seed, followed by a number, to initialize curand with a constant seed. "
+                         "(0 = random seed)"
+                      << std::endl;
+            std::cout << "Use -q or --query, followed by : number of simulation, time bound, a variable threshold, "
+                         "a variable name (id), Max=1 or Min=0, Estimate=1 or Probability=0."
+                      << std::endl;
+            return false;
+        } else {
+            std::cerr << "Error: unknown option: " << arg << std::endl;
+            return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+int main(int argc, char *argv[]) {
+    std::string filename = "../xml_files/LargeModels/aloha_50.xml";
+    int seed = 1235;
+    StatConfig st;
+    if (!handle_args(argc, argv, &filename, &seed, &st)) return 0;
+    const int rc = csmc_smc(filename.c_str(), seed, st.simulations, st.time_bound, st.threshold, st.var_id,
+                            st.is_max ? 1 : 0, st.is_estimate ? 1 : 0, st.loc_query.c_str());
+    if (rc != CSMC_OK) std::cerr << "Error: " << csmc_last_error() << std::endl;
+    return 1;
+}

@@ -1,0 +1,123 @@
+/*
+ * Packed network blob: the read-only structure-of-arrays image of one
+ * stochastic-timed-automata network that the simulation kernels stage into
+ * shared memory (and that the CPU oracle reads).  It replaces the reference's
+ * pointer-linked SharedModelState (simulation/state/shared_model_state.cuh:
+ * 45-217): destinations are local location indices instead of node ids found
+ * by scanning levels (simulation/simulation.cu:147-168), only the guards and
+ * invariants the kernel acts on are stored, and expressions are flat
+ * programs instead of 32-byte pointer-linked records.
+ *
+ * All sections start on 16-byte boundaries; all integers are little endian.
+ */
+#ifndef CSMC_NET_H
+#define CSMC_NET_H
+
+#include <stdint.h>
+
+#define CSMC_NET_MAGIC 0x314e4d43u /* "CMN1" */
+#define CSMC_NET_VERSION 1u
+
+/* Expression handle: two tag bits + 30-bit payload. */
+#define CSMC_H_LIT 0u  /* payload: index into consts[] */
+#define CSMC_H_VAR 1u  /* payload: variable id */
+#define CSMC_H_PN 2u   /* payload: start index into code[] (postfix program, reference PN semantics) */
+#define CSMC_H_TREE 3u /* payload: start index into code[] (tree-evaluator semantics) */
+#define CSMC_H_TAG(h) ((uint32_t)(h) >> 30)
+#define CSMC_H_PAYLOAD(h) ((uint32_t)(h)&0x3fffffffu)
+#define CSMC_H_MAKE(tag, p) (((uint32_t)(tag) << 30) | ((uint32_t)(p)&0x3fffffffu))
+
+/* Program instructions: one uint64, low 8 bits opcode, bits 8..31 operand a. */
+enum csmc_opcode {
+    CSMC_OP_END = 0,
+    CSMC_OP_PUSH_C,  /* a: const index */
+    CSMC_OP_PUSH_V,  /* a: variable id */
+    /* postfix (PN) operators: read the top entries WITHOUT popping them and
+       push the result (simulation/expressions.cu:88-173, stack_top is passed
+       by value) */
+    CSMC_OP_ADD, CSMC_OP_SUB, CSMC_OP_MUL, CSMC_OP_DIV, CSMC_OP_POW, CSMC_OP_NEG,
+    CSMC_OP_SQRT, CSMC_OP_MOD, CSMC_OP_AND, CSMC_OP_OR, CSMC_OP_LE, CSMC_OP_GE,
+    CSMC_OP_LT, CSMC_OP_GT, CSMC_OP_EQ, CSMC_OP_NE, CSMC_OP_NOT,
+    CSMC_OP_RANDOM, /* pushes 1.0 (unsupported in the reference kernel) */
+    CSMC_OP_DUP,    /* conditional record: pushes the top entry again */
+    CSMC_OP_ZERO,   /* compiled/pn records: push 0.0 */
+    CSMC_OP_SKIP,   /* a: length; pop one; if |v| > 1e-5 jump over a records */
+    /* tree-evaluator operators (simulation/expressions.cu:199-307): proper
+       pop-two push-one stack discipline */
+    CSMC_OP_TADD, CSMC_OP_TSUB, CSMC_OP_TMUL,
+    CSMC_OP_TDIV, /* r == 0 -> 0; result == 0 -> DBL_MIN */
+    CSMC_OP_COUNT
+};
+
+#define CSMC_INS(op, a) ((uint64_t)(op) | ((uint64_t)(a) << 8))
+#define CSMC_INS_OP(i) ((uint32_t)((i)&0xffu))
+#define CSMC_INS_A(i) ((uint32_t)(((i) >> 8) & 0xffffffu))
+
+/* Guard / invariant operators as stored. */
+enum csmc_gop { CSMC_G_LE = 0, CSMC_G_LT = 1, CSMC_G_GE = 2, CSMC_G_GT = 3, CSMC_G_EQ = 4, CSMC_G_FALSE = 5 };
+
+/* Location types (reference node::node_types, include/engine/domain.h:140-147). */
+enum csmc_loc_type { CSMC_LOC = 0, CSMC_GOAL = 1, CSMC_BRANCH = 2, CSMC_URGENT = 3, CSMC_COMMITTED = 4 };
+
+typedef struct {
+    uint32_t magic, version, total_bytes, header_bytes;
+    uint32_t n_comps, n_locs, n_edges, n_guards;
+    uint32_t n_updates, n_vars, n_consts, n_code;
+    uint32_t max_locs_per_comp, max_edges_per_loc, max_stack, n_clocks;
+    uint32_t off_comp, off_loc, off_edge, off_guard;
+    uint32_t off_update, off_var, off_const, off_code;
+    uint32_t n_channels_max, max_inv_per_loc, max_guards_per_edge, max_updates_per_edge;
+    uint32_t flags, reserved[3];
+} csmc_net_header; /* 128 bytes */
+
+typedef struct {
+    uint32_t loc_begin;  /* global index of the component's first location */
+    uint16_t n_locs;
+    uint16_t init_local; /* initial location, local index */
+} csmc_comp;             /* 8 bytes */
+
+typedef struct {
+    uint32_t edge_begin;
+    uint32_t inv_begin;  /* into guards[]: delay-bounding invariants only */
+    uint32_t rate;       /* expression handle of the exponential rate */
+    uint8_t type;        /* csmc_loc_type */
+    uint8_t n_edges;
+    uint8_t n_inv;
+    uint8_t n_recv;      /* number of receiving edges (channel < 0) */
+} csmc_loc;              /* 16 bytes */
+
+typedef struct {
+    int16_t dst_local;   /* -1: destination not in this component (no move) */
+    int16_t channel;     /* 0 tau, >0 broadcast sender, <0 receiver */
+    uint32_t weight;      /* expression handle (tree semantics) */
+    uint32_t guard_begin; /* guard_begin (24 bits) | n_guards << 24 */
+    uint32_t upd;         /* update_begin (24 bits) | n_updates << 24 */
+} csmc_edge; /* 16 bytes */
+
+#define CSMC_EDGE_GUARD_BEGIN(e) ((e).guard_begin & 0xffffffu)
+#define CSMC_EDGE_N_GUARDS(e) ((e).guard_begin >> 24)
+#define CSMC_EDGE_UPD_BEGIN(e) ((e).upd & 0xffffffu)
+#define CSMC_EDGE_N_UPD(e) ((e).upd >> 24)
+
+typedef struct {
+    uint16_t var;
+    uint8_t op;    /* csmc_gop */
+    uint8_t clock; /* 1 when var is a clock */
+    uint32_t rhs;  /* expression handle */
+} csmc_guard;      /* 8 bytes */
+
+typedef struct {
+    uint32_t var;
+    uint32_t expr; /* expression handle (PN semantics) */
+} csmc_update;     /* 8 bytes */
+
+typedef struct {
+    float init;    /* initial value (int-truncated, as the reference uploads it) */
+    uint32_t kind; /* 1 clock, 0 int */
+} csmc_var;        /* 8 bytes */
+
+/* Limits of the packed form. */
+#define CSMC_MAX_EDGES_PER_LOC 32 /* enabled-edge slot state is a 32-bit mask */
+#define CSMC_MAX_STACK 32         /* expression stack entries */
+
+#endif

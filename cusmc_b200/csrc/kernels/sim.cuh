@@ -1,0 +1,61 @@
+// Simulation kernel for sm_100a: the reference's per-run loop
+// (simulation/simulation.cu:674-901) re-mapped onto lane groups.
+//
+// Mapping.  One run is simulated by a group of G lanes (G a power of two,
+// G <= 32); lane l of a group owns components l*K .. l*K+K-1.  Several groups
+// share a warp when G < 32.  The packed network (read-only, a few KB to a few
+// hundred KB) is staged once per CTA into shared memory; each group keeps its
+// run's variables, broadcast channel, goal flag and query extrema in shared
+// memory, and each lane keeps its components' locations and enabled-edge slot
+// masks in registers.  There are no block-wide barriers in the loop: a step is
+//   1. broadcast receivers of the previous step's sender (enabled sets in
+//      parallel, transitions serially in component order);
+//   2. per-component delays (lane-parallel);
+//   3. the race: a segmented xor-butterfly min over (delay key, bit-reversed
+//      component index), which reproduces the reference's strided
+//      shared-memory tree argmin (simulation/simulation.cu:576-628) exactly,
+//      ties included;
+//   4. clock advance (lane-parallel over variables) and the winner's
+//      transition (one lane).
+// Runs are pulled from a device work counter, so groups whose runs end early
+// refill immediately (persistent kernel, grid = resident CTAs).
+#pragma once
+#include <cstdint>
+
+#include "../include/csmc_net.h"
+#include "../include/csmc_numeric.h"
+
+namespace csmc {
+
+struct SimParams {
+    const uint8_t *blob;       // packed network in global memory
+    uint32_t blob_bytes;       // bytes to stage (multiple of 16)
+    uint32_t state_stride;     // bytes of per-group run state in shared memory (multiple of 16)
+    int32_t loc_mode;          // CSMC_QUERY_LOCATION
+    int32_t var_id;            // tracked variable or -1
+    int32_t is_max;
+    int32_t pad0;
+    double threshold;
+    float horizon;             // time bound as the reference's float time_bound
+    uint32_t pad1;
+    uint64_t max_steps;
+    uint64_t seed;
+    uint64_t first_run;
+    uint64_t n_runs;
+    uint8_t *flags;            // per-run outputs (may be null)
+    double *values;
+    uint32_t *steps;
+    uint64_t *digests;         // verification outputs (may be null)
+    uint32_t *final_state;
+    unsigned long long *scratch;  // [0] work counter [1] hits [2] steps [3] capped [4] errors
+};
+
+#define CSMC_SCRATCH_WORDS 8
+
+// Launch entry points (defined in sim_kernel.cu).
+int sim_launch(int lanes_per_run, int comps_per_lane, bool verify, const SimParams &p, int grid, int block,
+               size_t smem, void *stream);
+int sim_max_active_ctas(int lanes_per_run, int comps_per_lane, bool verify, int block, size_t smem, int *ctas);
+bool sim_supported(int lanes_per_run, int comps_per_lane);
+
+}  // namespace csmc

@@ -1,0 +1,6 @@
+// Kernel instantiations for lane-group shapes: 32,8
+#include "sim_impl.cuh"
+
+namespace csmc {
+CSMC_INSTANTIATE_SHAPE(32, 8)
+}  // namespace csmc

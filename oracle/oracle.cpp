@@ -1,0 +1,490 @@
+/*
+ * CPU oracle — TEST INFRASTRUCTURE ONLY.  A single-threaded restatement of
+ * the reference cuSMC simulation semantics over the packed network, used by
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the
+ * checker.  Nothing in the product (cusmc_b200, the CLI, libcsmc.so) links,
+ * loads or calls it.
+ *
+ * Parity status: the front end that produces the packed network is pinned
+ * byte-for-byte against the reference's own parser and passes (oracle/ref/
+ * refdump.cpp, tests/golden/frontend).  The simulation semantics below
+ * restate the reference kernel; they are pinned statistically against the
+ * reference binary run on the GPU (tests/golden/ref_estimates.json) and by
+ * closed forms.  The reference draws from curand states shared across blocks
+ * (simulation/simulation.cu:756-760, smc.cu:228), so its runs have no
+ * reproducible traces to compare bit for bit; traces are compared bit for bit
+ * between this oracle and the CUDA kernels, which share only the numeric
+ * spec of cusmc_b200/csrc/include/csmc_numeric.h.
+ *
+ * Step semantics followed (simulation/simulation.cu):
+ *   loop / goal exit / time advance ............ 835-885
+ *   broadcast receivers (serial, in order) ...... 357-407
+ *   delay per component ......................... 409-541
+ *   race: tree argmin, clock advance, winner .... 544-671
+ *   edge enabling / guards ...................... 184-305
+ *   edge choice, updates, destination, goal ..... 9-181
+ *   per-run output ............................... 887-893
+ * Expression evaluation: simulation/expressions.cu:88-229.
+ */
+#include "../include/csmc.h"
+#include "../cusmc_b200/csrc/include/csmc_net.h"
+#include "../cusmc_b200/csrc/include/csmc_numeric.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace csmc;
+
+namespace {
+
+thread_local std::string g_err;
+
+constexpr double kEps = 0.00001;
+constexpr double kDblMax = 1.7976931348623158e+308;
+constexpr double kDblMin = 2.2250738585072014e-308;
+
+struct Net {
+    const csmc_net_header *h;
+    const csmc_comp *comp;
+    const csmc_loc *loc;
+    const csmc_edge *edge;
+    const csmc_guard *guard;
+    const csmc_update *upd;
+    const csmc_var *var;
+    const double *konst;
+    const uint64_t *code;
+};
+
+Net view(const void *blob, size_t bytes) {
+    if (!blob || bytes < sizeof(csmc_net_header)) throw std::runtime_error("blob too small");
+    const uint8_t *b = static_cast<const uint8_t *>(blob);
+    Net n;
+    n.h = reinterpret_cast<const csmc_net_header *>(b);
+    if (n.h->magic != CSMC_NET_MAGIC || n.h->total_bytes > bytes) throw std::runtime_error("not a network blob");
+    n.comp = reinterpret_cast<const csmc_comp *>(b + n.h->off_comp);
+    n.loc = reinterpret_cast<const csmc_loc *>(b + n.h->off_loc);
+    n.edge = reinterpret_cast<const csmc_edge *>(b + n.h->off_edge);
+    n.guard = reinterpret_cast<const csmc_guard *>(b + n.h->off_guard);
+    n.upd = reinterpret_cast<const csmc_update *>(b + n.h->off_update);
+    n.var = reinterpret_cast<const csmc_var *>(b + n.h->off_var);
+    n.konst = reinterpret_cast<const double *>(b + n.h->off_const);
+    n.code = reinterpret_cast<const uint64_t *>(b + n.h->off_code);
+    return n;
+}
+
+struct Digest {
+    uint64_t h = 0xcbf29ce484222325ull;
+    void mix(uint32_t w) { h = (h ^ w) * 0x100000001b3ull; }
+};
+
+class Run {
+  public:
+    Run(const Net &n, const csmc_query &q, uint64_t seed, uint64_t run) : n_(n), q_(q), seed_(seed), run_(run) {}
+
+    // expressions.cu:175-197 (PN, stack never popped by operators) and
+    // expressions.cu:199-307 (tree evaluator)
+    double eval(uint32_t h) const {
+        const uint32_t tag = CSMC_H_TAG(h), p = CSMC_H_PAYLOAD(h);
+        if (tag == CSMC_H_LIT) return n_.konst[p];
+        if (tag == CSMC_H_VAR) return static_cast<double>(vars_[p]);
+        double st[CSMC_MAX_STACK + 2];
+        int top = 0;
+        for (uint32_t ip = p;; ++ip) {
+            const uint64_t ins = n_.code[ip];
+            const uint32_t op = CSMC_INS_OP(ins), a = CSMC_INS_A(ins);
+            double v1 = top >= 2 ? st[top - 2] : 0.0, v2 = top >= 1 ? st[top - 1] : 0.0;
+            double r;
+            switch (op) {
+            case CSMC_OP_END: return top > 0 ? st[top - 1] : 0.0;
+            case CSMC_OP_PUSH_C: r = n_.konst[a]; break;
+            case CSMC_OP_PUSH_V: r = static_cast<double>(vars_[a]); break;
+            case CSMC_OP_ADD: r = v1 + v2; break;
+            case CSMC_OP_SUB: r = v1 - v2; break;
+            case CSMC_OP_MUL: r = v1 * v2; break;
+            case CSMC_OP_DIV: r = v1 / v2; break;
+            case CSMC_OP_POW: r = pow_model(v1, v2); break;
+            case CSMC_OP_NEG: r = -v2; break;
+            case CSMC_OP_SQRT: r = std::sqrt(v2); break;
+            case CSMC_OP_MOD: {
+                const int x = d2i_sat(v1), y = d2i_sat(v2 + kEps);
+                r = (y == 0 || (x == (-2147483647 - 1) && y == -1)) ? 0.0 : static_cast<double>(x % y);
+                break;
+            }
+            case CSMC_OP_AND: r = (std::fabs(v1) > kEps && std::fabs(v2) > kEps) ? 1.0 : 0.0; break;
+            case CSMC_OP_OR: r = (std::fabs(v1) > kEps || std::fabs(v2) > kEps) ? 1.0 : 0.0; break;
+            case CSMC_OP_LE: r = v1 <= v2 ? 1.0 : 0.0; break;
+            case CSMC_OP_GE: r = v1 >= v2 ? 1.0 : 0.0; break;
+            case CSMC_OP_LT: r = v1 < v2 ? 1.0 : 0.0; break;
+            case CSMC_OP_GT: r = v1 > v2 ? 1.0 : 0.0; break;
+            case CSMC_OP_EQ: r = std::fabs(v1 - v2) <= kEps ? 1.0 : 0.0; break;
+            case CSMC_OP_NE: r = std::fabs(v1 - v2) > kEps ? 1.0 : 0.0; break;
+            case CSMC_OP_NOT: r = std::fabs(v2) < kEps ? 1.0 : 0.0; break;
+            case CSMC_OP_RANDOM: r = 1.0; break;
+            case CSMC_OP_DUP: r = v2; break;
+            case CSMC_OP_ZERO: r = 0.0; break;
+            case CSMC_OP_SKIP: {
+                --top;
+                if (std::fabs(st[top]) > kEps) ip += a;
+                continue;
+            }
+            case CSMC_OP_TADD: case CSMC_OP_TSUB: case CSMC_OP_TMUL: case CSMC_OP_TDIV: {
+                const double R = st[--top], L = st[--top];
+                if (op == CSMC_OP_TADD) r = L + R;
+                else if (op == CSMC_OP_TSUB) r = L - R;
+                else if (op == CSMC_OP_TMUL) r = L * R;
+                else if (R == 0.0) r = 0.0;
+                else {
+                    r = L / R;
+                    if (r == 0.0) r = kDblMin;
+                }
+                break;
+            }
+            default: throw std::runtime_error("bad opcode");
+            }
+            st[top++] = r;
+        }
+    }
+
+    // simulation.cu:184-266
+    bool guards_ok(const csmc_edge &e) const {
+        const uint32_t gb = CSMC_EDGE_GUARD_BEGIN(e), ng = CSMC_EDGE_N_GUARDS(e);
+        for (uint32_t i = 0; i < ng; ++i) {
+            const csmc_guard &g = n_.guard[gb + i];
+            const double v = static_cast<double>(vars_[g.var]);
+            const double b = eval(g.rhs);
+            bool ok;
+            switch (g.op) {
+            case CSMC_G_LT: ok = v < b; break;
+            case CSMC_G_LE: ok = v <= b; break;
+            case CSMC_G_GT: ok = v > b; break;
+            case CSMC_G_GE: ok = v >= b; break;
+            case CSMC_G_EQ: ok = std::fabs(v - b) <= kEps; break;
+            default: ok = false; break;
+            }
+            if (!ok) return false;
+        }
+        return true;
+    }
+
+    // simulation.cu:409-541
+    float delay(uint32_t c) const {
+        const csmc_loc &L = n_.loc[n_.comp[c].loc_begin + loc_[c]];
+        if (L.type > 1) return 0.0f;
+        double max_delay = kDblMax;
+        bool bounded = false;
+        for (uint32_t i = 0; i < L.n_inv; ++i) {
+            const csmc_guard &g = n_.guard[L.inv_begin + i];
+            const double cur = static_cast<double>(vars_[g.var]);
+            const double bound = eval(g.rhs);
+            double ttb = bound - cur;
+            if (g.op == CSMC_G_LT) ttb -= 1e-6;
+            if (ttb >= 0) {
+                max_delay = std::fmin(max_delay, ttb);
+                bounded = true;
+            }
+        }
+        const uint32_t x = delay_word(seed_, run_, step_, c);
+        if (bounded) return uniform_delay(x, max_delay);
+        return exp_delay(x, eval(L.rate));
+    }
+
+    // simulation.cu:9-24 and 27-181.  en: enabled edge indices (ascending).
+    void take(uint32_t c, const std::vector<uint32_t> &en, uint32_t choice_which) {
+        const uint32_t n = static_cast<uint32_t>(en.size());
+        if (n == 0) return;
+        const csmc_loc &L = n_.loc[n_.comp[c].loc_begin + loc_[c]];
+        uint32_t sel = en[0];
+        if (n > 1) {
+            double sum = 0;
+            for (uint32_t i = 0; i < L.n_edges; ++i)
+                if ((mask_[c] >> i) & 1u) sum += eval(n_.edge[L.edge_begin + i].weight);
+            const int W = d2i_sat(sum);
+            const float u = uniform01(choice_word(seed_, run_, step_, c, choice_which));
+            const int rnd = f2i_sat(f_mul(static_cast<float>(W), u));
+            uint32_t temp = static_cast<uint32_t>(W);
+            for (int i = static_cast<int>(n) - 1; i >= 0; --i) {
+                const int w = d2i_sat(eval(n_.edge[L.edge_begin + i].weight));
+                if (static_cast<int>(temp - static_cast<uint32_t>(w)) <= rnd) {
+                    sel = en[i];
+                    break;
+                }
+                temp -= static_cast<uint32_t>(w);
+            }
+        }
+        if (digest_) {
+            dg_.mix(sel);
+        }
+        const csmc_edge &e = n_.edge[L.edge_begin + sel];
+        if (e.channel > 0) {
+            chan_ = e.channel;
+            sender_ = static_cast<int>(c);
+        }
+        const uint32_t ub = CSMC_EDGE_UPD_BEGIN(e), nu = CSMC_EDGE_N_UPD(e);
+        for (uint32_t i = 0; i < nu; ++i) {
+            const csmc_update &u = n_.upd[ub + i];
+            const double nv = eval(u.expr);
+            if (static_cast<int32_t>(u.var) == q_.var_id) {
+                if (nv > qmax_) qmax_ = nv;
+                if (nv < qmin_) qmin_ = nv;
+            }
+            vars_[u.var] = d2f(nv);
+            if (digest_) {
+                dg_.mix(u.var);
+                dg_.mix(f_bits(vars_[u.var]));
+            }
+        }
+        if (e.dst_local < 0) return;
+        loc_[c] = static_cast<uint16_t>(e.dst_local);
+        if (n_.loc[n_.comp[c].loc_begin + loc_[c]].type == CSMC_GOAL) goal_ = true;
+    }
+
+    // enabled-edge slot state: bit i <=> slot i holds edge index i
+    void write_slots(uint32_t c, const std::vector<uint32_t> &en) {
+        uint32_t m = mask_[c];
+        for (uint32_t i = 0; i < en.size() && i < 32; ++i) {
+            if (en[i] == i) m |= 1u << i;
+            else m &= ~(1u << i);
+        }
+        mask_[c] = m;
+    }
+
+    void simulate(bool digest) {
+        digest_ = digest;
+        const uint32_t C = n_.h->n_comps, V = n_.h->n_vars;
+        vars_.resize(V);
+        for (uint32_t v = 0; v < V; ++v) vars_[v] = n_.var[v].init;
+        loc_.resize(C);
+        mask_.assign(C, 0u);
+        for (uint32_t c = 0; c < C; ++c) loc_[c] = n_.comp[c].init_local;
+        qmin_ = qmax_ = 0.0;
+        if (q_.var_id >= 0 && static_cast<uint32_t>(q_.var_id) < V && n_.var[q_.var_id].kind == 0)
+            qmin_ = qmax_ = static_cast<double>(n_.var[q_.var_id].init);
+        const float T = static_cast<float>(q_.horizon);
+        const uint64_t cap = q_.max_steps ? q_.max_steps : 0xffffffffull;
+        const bool loc_mode = q_.kind == CSMC_QUERY_LOCATION;
+        const uint32_t bits = ceil_log2(C);
+        std::vector<float> d(C);
+        std::vector<uint32_t> keys(C), idx(C);
+        std::vector<std::vector<uint32_t>> recv(C);
+        std::vector<uint32_t> en;
+        float time = 0.0f;
+        while (time < T) {
+            if (goal_ && loc_mode) {
+                flag_ = 1;
+                break;
+            }
+            if (step_ >= cap) {
+                capped_ = true;
+                break;
+            }
+            // broadcast receivers: enabled sets first, then serial transitions
+            if (chan_ > 0) {
+                for (uint32_t c = 0; c < C; ++c) {
+                    recv[c].clear();
+                    if (static_cast<int>(c) == sender_) continue;
+                    const csmc_loc &L = n_.loc[n_.comp[c].loc_begin + loc_[c]];
+                    for (uint32_t i = 0; i < L.n_edges; ++i) {
+                        const csmc_edge &e = n_.edge[L.edge_begin + i];
+                        if (e.channel == -chan_ && guards_ok(e)) recv[c].push_back(i);
+                    }
+                }
+                for (uint32_t c = 0; c < C; ++c) {
+                    if (recv[c].empty()) continue;
+                    write_slots(c, recv[c]);
+                    if (digest_) dg_.mix(c | 0x80000000u);
+                    take(c, recv[c], 1);
+                }
+                chan_ = 0;
+                sender_ = -1;
+            }
+            for (uint32_t c = 0; c < C; ++c) {
+                d[c] = delay(c);
+                keys[c] = delay_key(d[c]);
+                idx[c] = c;
+            }
+            // the reference's tree reduction (simulation.cu:576-628)
+            uint32_t P = 1u << bits;
+            for (uint32_t stride = P / 2; stride > 0; stride >>= 1)
+                for (uint32_t t = 0; t < stride; ++t) {
+                    const uint32_t j = t + stride;
+                    if (j < C && keys[j] < keys[t]) {
+                        keys[t] = keys[j];
+                        idx[t] = idx[j];
+                    }
+                }
+            const uint32_t win = idx[0];
+            const float dmin = d[win];
+            if (digest_) {
+                dg_.mix(step_);
+                dg_.mix(win);
+                dg_.mix(f_bits(dmin));
+            }
+            if (static_cast<double>(dmin) < kDblMax) {
+                for (uint32_t v = 0; v < V; ++v)
+                    if (n_.var[v].kind) vars_[v] = d2f(static_cast<double>(vars_[v]) + static_cast<double>(dmin));
+                const csmc_loc &L = n_.loc[n_.comp[win].loc_begin + loc_[win]];
+                en.clear();
+                for (uint32_t i = 0; i < L.n_edges; ++i) {
+                    const csmc_edge &e = n_.edge[L.edge_begin + i];
+                    if (e.channel >= 0 && guards_ok(e)) en.push_back(i);
+                }
+                write_slots(win, en);
+                if (en.empty() && digest_) dg_.mix(0xffffffffu);
+                take(win, en, 0);
+            }
+            time = d2f(static_cast<double>(time) + static_cast<double>(dmin));
+            ++step_;
+        }
+        time_ = time;
+    }
+
+    uint8_t flag_ = 0;
+    bool capped_ = false;
+    uint32_t step_ = 0;
+    double qmin_ = 0, qmax_ = 0;
+    float time_ = 0;
+    std::vector<float> vars_;
+    std::vector<uint16_t> loc_;
+    uint64_t digest() const { return dg_.h; }
+
+  private:
+    const Net &n_;
+    const csmc_query &q_;
+    uint64_t seed_, run_;
+    std::vector<uint32_t> mask_;
+    bool goal_ = false;
+    int chan_ = 0, sender_ = -1;
+    bool digest_ = false;
+    Digest dg_;
+};
+
+}  // namespace
+
+extern "C" {
+
+const char *oracle_last_error(void) { return g_err.c_str(); }
+
+/* Simulates runs with the reference semantics on `threads` host threads
+ * (<= 0: all hardware threads).  Per-run outputs (host, may be NULL): flags,
+ * values, steps, digests, final_state (n_comps + n_vars words per run).
+ * wall_ms (may be NULL) receives the time spent in the run loop. */
+int oracle_run(const void *blob, size_t bytes, const csmc_query *q, uint64_t seed, uint64_t first_run,
+               uint64_t n_runs, int threads, uint8_t *flags, double *values, uint32_t *steps, uint64_t *digests,
+               uint32_t *final_state, csmc_result *out, double *wall_ms) {
+    try {
+        if (!q) throw std::runtime_error("null query");
+        const Net n = view(blob, bytes);
+        const uint32_t C = n.h->n_comps, V = n.h->n_vars;
+        if (q->kind == CSMC_QUERY_VARIABLE && (q->var_id < 0 || static_cast<uint32_t>(q->var_id) >= V))
+            throw std::runtime_error("query variable id out of range");
+        int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+        if (nt < 1) nt = 1;
+        if (static_cast<uint64_t>(nt) > n_runs) nt = static_cast<int>(std::max<uint64_t>(1, n_runs));
+        std::vector<uint8_t> f(n_runs);
+        std::vector<double> val(n_runs);
+        std::vector<uint32_t> st(n_runs);
+        std::vector<uint8_t> cap(n_runs);
+        std::atomic<uint64_t> next{0};
+        const bool want_digest = digests != nullptr;
+        auto worker = [&]() {
+            for (;;) {
+                const uint64_t i = next.fetch_add(1);
+                if (i >= n_runs) break;
+                Run r(n, *q, seed, first_run + i);
+                r.simulate(want_digest);
+                const double v = q->is_max ? r.qmax_ : r.qmin_;
+                uint8_t fl;
+                if (q->kind == CSMC_QUERY_LOCATION) fl = r.flag_;
+                else fl = q->is_max ? (v > q->threshold) : (v < q->threshold);
+                f[i] = fl;
+                val[i] = v;
+                st[i] = r.step_;
+                cap[i] = r.capped_ ? 1 : 0;
+                if (digests) digests[i] = r.digest();
+                if (final_state) {
+                    uint32_t *w = final_state + i * (C + V);
+                    for (uint32_t c = 0; c < C; ++c) w[c] = r.loc_[c];
+                    for (uint32_t v2 = 0; v2 < V; ++v2) w[C + v2] = f_bits(r.vars_[v2]);
+                }
+            }
+        };
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto &t : pool) t.join();
+        const auto t1 = std::chrono::steady_clock::now();
+        if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        csmc_result res;
+        std::memset(&res, 0, sizeof res);
+        res.runs = n_runs;
+        for (uint64_t i = 0; i < n_runs; ++i) {
+            res.hits += f[i];
+            res.steps += st[i];
+            res.capped += cap[i];
+            res.sum += val[i];
+            res.sum_sq += val[i] * val[i];
+        }
+        if (n_runs) {
+            if (q->kind == CSMC_QUERY_VARIABLE && q->is_estimate) res.estimate = res.sum / static_cast<double>(n_runs);
+            else res.estimate = static_cast<double>(res.hits) / static_cast<double>(n_runs);
+        }
+        if (flags) std::memcpy(flags, f.data(), n_runs);
+        if (values) std::memcpy(values, val.data(), n_runs * sizeof(double));
+        if (steps) std::memcpy(steps, st.data(), n_runs * sizeof(uint32_t));
+        if (out) *out = res;
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return CSMC_ERR_ARG;
+    }
+}
+
+/* Full state after every step of one run: per step
+ * [step, winner, delay bits, time bits, locations..., variable bits...]. */
+int oracle_trace(const void *blob, size_t bytes, const csmc_query *q, uint64_t seed, uint64_t run,
+                 uint32_t *rec, size_t cap_steps, size_t *n_steps) {
+    try {
+        const Net n = view(blob, bytes);
+        csmc_query qq = *q;
+        size_t k = 0;
+        const uint32_t C = n.h->n_comps, V = n.h->n_vars;
+        const size_t W = 4 + C + V;
+        for (uint64_t s = 1;; ++s) {
+            qq.max_steps = s;
+            Run r(n, qq, seed, run);
+            r.simulate(false);
+            if (r.step_ < s || !r.capped_) {  // run ended before step s
+                *n_steps = k;
+                return CSMC_OK;
+            }
+            if (k < cap_steps) {
+                uint32_t *w = rec + k * W;
+                w[0] = static_cast<uint32_t>(s - 1);
+                w[1] = 0;
+                w[2] = 0;
+                w[3] = f_bits(r.time_);
+                for (uint32_t c = 0; c < C; ++c) w[4 + c] = r.loc_[c];
+                for (uint32_t v = 0; v < V; ++v) w[4 + C + v] = f_bits(r.vars_[v]);
+            }
+            ++k;
+            if (k >= cap_steps) {
+                *n_steps = k;
+                return CSMC_OK;
+            }
+        }
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return CSMC_ERR_ARG;
+    }
+}
+
+}  // extern "C"

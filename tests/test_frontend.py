@@ -1,0 +1,85 @@
+"""Front-end parity: this library's front end against the REFERENCE front end
+(parser, optimizer, PN compiler, variable registry, location-query goal
+marking), compared on the canonical dump of the network each delivers to its
+kernel.  The reference side is committed under tests/golden/frontend (made by
+tests/golden/make_golden.py from oracle/_ref/refdump).
+"""
+import gzip
+import json
+import os
+import tempfile
+
+import pytest
+
+from conftest import GOLDEN
+from cusmc_b200 import api, netgen
+
+REF_XML = "/root/reference/xml_files"
+
+with open(os.path.join(GOLDEN, "manifest.json")) as f:
+    MANIFEST = json.load(f)
+
+
+def _golden(name, mode):
+    with gzip.open(os.path.join(GOLDEN, "frontend", f"{name}.{mode}.dump.gz"), "rt") as f:
+        return f.read()
+
+
+def _generated():
+    ws = {w.name: w for w in [netgen.epidemic(), netgen.mutex(8), netgen.mutex(32)]}
+    ws.update({w.name: w for w in [netgen.random_network(s) for s in range(4)]})
+    ws.update({w.name: w for w in netgen.batch_networks(6)})
+    return ws
+
+
+GENERATED = _generated()
+
+
+@pytest.mark.parametrize("entry", [m for m in MANIFEST["models"] if m["generated"]],
+                         ids=lambda m: f"{m['name']}-{m['mode']}")
+def test_generated_models_match_reference_front_end(entry):
+    w = GENERATED[entry["name"]]
+    with tempfile.NamedTemporaryFile("w", suffix=".xml", delete=False) as f:
+        f.write(w.xml)
+        path = f.name
+    try:
+        got = api.dump_model(path, entry["loc_query"], entry["mode"] == "loc")
+    finally:
+        os.unlink(path)
+    assert got == _golden(entry["name"], entry["mode"])
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_XML), reason="reference model files not present")
+@pytest.mark.parametrize("entry", [m for m in MANIFEST["models"] if not m["generated"]],
+                         ids=lambda m: f"{m['name']}-{m['mode']}")
+def test_reference_fixtures_match_reference_front_end(entry):
+    name = entry["name"]
+    rel = name + ".xml"
+    path = os.path.join(REF_XML, rel)
+    if not os.path.exists(path):
+        path = os.path.join(REF_XML, "LargeModels", rel)
+    got = api.dump_model(path, entry["loc_query"], entry["mode"] == "loc")
+    assert got == _golden(name, entry["mode"])
+    blob = api.compile_model(path, entry["loc_query"], entry["mode"] == "loc")
+    with open(os.path.join(GOLDEN, "nets", f"{name}.{entry['mode']}.blob"), "rb") as f:
+        assert blob == f.read()
+
+
+def test_unreachable_location_is_rejected_like_the_reference():
+    # the reference's upload throws std::out_of_range for a location that the
+    # optimizer never visited (shared_model_state.cu:475)
+    xml = netgen.epidemic(n_agents=3).xml.replace('<init ref="id0"/>', '<init ref="id1"/>', 1)
+    with tempfile.NamedTemporaryFile("w", suffix=".xml", delete=False) as f:
+        f.write(xml)
+        path = f.name
+    try:
+        with pytest.raises(api._native.CsmcError):
+            api.compile_model(path)
+    finally:
+        os.unlink(path)
+
+
+def test_missing_file_is_a_model_error():
+    with pytest.raises(api._native.CsmcError) as e:
+        api.compile_model("/nonexistent/model.xml")
+    assert e.value.code == api._native.CSMC_ERR_MODEL
