@@ -137,7 +137,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     w, path, blob, q = epidemic_blob()
     net = api.Network(blob)
-    n = RUNS_PER_STEP
+    n = args.runs
     dev = torch.device("cuda", local)
     flags = torch.empty(n, dtype=torch.uint8, device=dev)
     values = torch.empty(n, dtype=torch.float64, device=dev)
@@ -211,7 +211,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 expressions", "data": "synthetic (seeded generated network)",
         "config": {"workload": "epidemic_100 (SEIR, 100 agents, beta=0.3, E->I 0.2, I->R 0.1), T=100, "
-                               "Pr[<=100](<> R>=50), 1e6 runs per step per GPU",
+                               f"Pr[<=100](<> R>=50), {n} runs per step per GPU",
                    "runs_per_step_per_gpu": n, "lanes_per_run": lanes, "comps_per_lane": cpl,
                    "runs_per_cta": rpc, "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"runs sharded over {world} GPU(s)"},
@@ -302,6 +302,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline")
+    ap.add_argument("--runs", type=int, default=RUNS_PER_STEP,
+                    help="runs per step per GPU (default 1e6; smaller values are for profiling captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -10,7 +10,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcsmc.so")
+# CSMC_LIBRARY selects another build of the library (for comparing builds).
+LIB_PATH = os.environ.get("CSMC_LIBRARY") or os.path.join(_HERE, "libcsmc.so")
 
 CSMC_OK = 0
 CSMC_ERR_ARG = -1

@@ -323,7 +323,9 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     choose_shape(h->n_comps, n->lanes, n->comps_per_lane);
     if (!csmc::sim_supported(n->lanes, n->comps_per_lane))
         return fail(CSMC_ERR_LIMIT, "networks with more than 1024 components are not supported");
-    n->state_stride = static_cast<uint32_t>((48 + 4 * h->n_vars + 15) & ~15u);
+    // per-group run state: 48 bytes of scalars, the variables, then one
+    // inverse rate per rate program (evaluated once per step)
+    n->state_stride = static_cast<uint32_t>((48 + 4 * (h->n_vars + h->n_rate_prog) + 15) & ~15u);
     n->smem = n->bytes + static_cast<size_t>(n->block / n->lanes) * n->state_stride;
     int max_smem = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device), "attribute");

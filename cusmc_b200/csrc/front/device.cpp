@@ -10,6 +10,7 @@
 //   device layout choices:  simulation/state/shared_model_state.cu:164-614
 #include "front.h"
 #include "../include/csmc_net.h"
+#include "../include/csmc_numeric.h"
 
 #include <algorithm>
 #include <cmath>
@@ -639,6 +640,39 @@ class Packer {
             if (v.kind) ++h.n_clocks;
             vars_.push_back(v);
         }
+        // rate slots: literal rates pre-inverted on the host, other rate
+        // expressions deduplicated into a per-step program table
+        std::vector<uint16_t> loc_rate;
+        std::vector<float> inv_lit;
+        std::vector<uint32_t> rate_prog;
+        {
+            std::map<uint32_t, uint16_t> lit_slot, prog_slot;
+            for (const csmc_loc &pl : locs_) {
+                const uint32_t hdl = pl.rate;
+                if (CSMC_H_TAG(hdl) == CSMC_H_LIT) {
+                    const float inv = csmc::inv_rate(consts_[CSMC_H_PAYLOAD(hdl)]);
+                    uint32_t bits;
+                    std::memcpy(&bits, &inv, 4);
+                    auto it = lit_slot.find(bits);
+                    if (it == lit_slot.end()) {
+                        it = lit_slot.emplace(bits, static_cast<uint16_t>(inv_lit.size())).first;
+                        inv_lit.push_back(inv);
+                    }
+                    loc_rate.push_back(it->second);
+                } else {
+                    auto it = prog_slot.find(hdl);
+                    if (it == prog_slot.end()) {
+                        it = prog_slot.emplace(hdl, static_cast<uint16_t>(rate_prog.size())).first;
+                        rate_prog.push_back(hdl);
+                    }
+                    loc_rate.push_back(static_cast<uint16_t>(it->second | CSMC_RATE_PROG_BIT));
+                }
+            }
+            if (inv_lit.size() >= CSMC_RATE_PROG_BIT) fail("too many distinct rates");
+            h.n_rate_prog = static_cast<uint32_t>(rate_prog.size());
+            h.n_inv_lit = static_cast<uint32_t>(inv_lit.size());
+            if (h.n_rate_prog <= CSMC_MAX_RATE_PROGS) h.flags |= CSMC_NET_RATE_TABLE;
+        }
         h.magic = CSMC_NET_MAGIC;
         h.version = CSMC_NET_VERSION;
         h.header_bytes = sizeof(csmc_net_header);
@@ -666,6 +700,9 @@ class Packer {
         h.off_var = section(vars_.data(), vars_.size() * sizeof(csmc_var));
         h.off_const = section(consts_.data(), consts_.size() * sizeof(double));
         h.off_code = section(code_.data(), code_.size() * sizeof(uint64_t));
+        h.off_loc_rate = section(loc_rate.data(), loc_rate.size() * sizeof(uint16_t));
+        h.off_inv_lit = section(inv_lit.data(), inv_lit.size() * sizeof(float));
+        h.off_rate_prog = section(rate_prog.data(), rate_prog.size() * sizeof(uint32_t));
         while (out.size() % 16) out.push_back(0);
         h.total_bytes = static_cast<uint32_t>(out.size());
         std::memcpy(out.data(), &h, sizeof h);
@@ -757,7 +794,8 @@ class Packer {
         return static_cast<uint32_t>(var);
     }
 
-    uint32_t program(std::vector<uint64_t> p, uint32_t tag) {
+    uint32_t program(std::vector<uint64_t> p, uint32_t tag, uint32_t flags, uint32_t depth) {
+        p.insert(p.begin(), CSMC_INS(CSMC_OP_HDR, flags | (depth << 8)));
         p.push_back(CSMC_INS(CSMC_OP_END, 0));
         std::vector<uint64_t> key = p;
         key.push_back(tag);
@@ -774,6 +812,7 @@ class Packer {
     uint32_t pn_program(const std::vector<Expr> &pn, uint32_t nv) {
         std::vector<uint64_t> p;
         uint32_t pushes = 0;
+        bool window = true;
         for (const Expr &r : pn) {
             uint32_t op;
             uint32_t a = 0;
@@ -803,13 +842,14 @@ class Packer {
             default: op = CSMC_OP_ZERO; break;
             }
             if (op != CSMC_OP_SKIP) ++pushes;
+            else window = false;
             p.push_back(CSMC_INS(op, a));
         }
         if (pushes > CSMC_MAX_STACK)
             fail("expression needs " + std::to_string(pushes) + " stack entries (limit " +
                  std::to_string(CSMC_MAX_STACK) + "; the reference kernel overflows beyond 10)");
         max_stack_ = std::max(max_stack_, pushes);
-        return program(p, CSMC_H_PN);
+        return program(p, CSMC_H_PN, window ? CSMC_PROG_WINDOW : 0u, pushes);
     }
 
     // Tree -> postfix with the recursive evaluator's semantics.
@@ -845,7 +885,7 @@ class Packer {
             tree_emit(d.tree, p, nv, 0, maxd);
             if (maxd > CSMC_MAX_STACK) fail("expression tree too deep");
             max_stack_ = std::max(max_stack_, maxd);
-            return CSMC_H_MAKE(CSMC_H_TREE, program(p, CSMC_H_TREE));
+            return CSMC_H_MAKE(CSMC_H_TREE, program(p, CSMC_H_TREE, maxd <= 2 ? CSMC_PROG_WINDOW : 0u, maxd));
         }
         }
     }

@@ -27,7 +27,9 @@
 #define CSMC_H_PAYLOAD(h) ((uint32_t)(h)&0x3fffffffu)
 #define CSMC_H_MAKE(tag, p) (((uint32_t)(tag) << 30) | ((uint32_t)(p)&0x3fffffffu))
 
-/* Program instructions: one uint64, low 8 bits opcode, bits 8..31 operand a. */
+/* Program instructions: one uint64, low 8 bits opcode, bits 8..31 operand a.
+ * Every program starts with a CSMC_OP_HDR instruction whose operand holds
+ * CSMC_PROG_* flags and the stack depth the program needs. */
 enum csmc_opcode {
     CSMC_OP_END = 0,
     CSMC_OP_PUSH_C,  /* a: const index */
@@ -46,8 +48,14 @@ enum csmc_opcode {
        pop-two push-one stack discipline */
     CSMC_OP_TADD, CSMC_OP_TSUB, CSMC_OP_TMUL,
     CSMC_OP_TDIV, /* r == 0 -> 0; result == 0 -> DBL_MIN */
+    CSMC_OP_HDR,  /* program header: a = flags | depth << 8 */
     CSMC_OP_COUNT
 };
+
+/* Program header flags.  WINDOW: the program only ever reads the two top
+ * stack entries (postfix programs without skips, trees of depth <= 2), so it
+ * can be evaluated with two registers. */
+#define CSMC_PROG_WINDOW 1u
 
 #define CSMC_INS(op, a) ((uint64_t)(op) | ((uint64_t)(a) << 8))
 #define CSMC_INS_OP(i) ((uint32_t)((i)&0xffu))
@@ -67,8 +75,24 @@ typedef struct {
     uint32_t off_comp, off_loc, off_edge, off_guard;
     uint32_t off_update, off_var, off_const, off_code;
     uint32_t n_channels_max, max_inv_per_loc, max_guards_per_edge, max_updates_per_edge;
-    uint32_t flags, reserved[3];
-} csmc_net_header; /* 128 bytes */
+    uint32_t flags;          /* CSMC_NET_* */
+    uint32_t n_rate_prog;    /* distinct non-literal rate expressions */
+    uint32_t n_inv_lit;      /* distinct literal rates (pre-inverted) */
+    uint32_t off_loc_rate;   /* uint16 per location: rate slot */
+    uint32_t off_inv_lit;    /* float per literal rate: 1/rate (inv_rate of csmc_numeric.h) */
+    uint32_t off_rate_prog;  /* uint32 expression handle per rate program */
+    uint32_t reserved[6];
+} csmc_net_header; /* 160 bytes */
+
+/* Header flags. */
+#define CSMC_NET_RATE_TABLE 1u /* rates resolved through loc_rate (see below) */
+
+/* Rate slot of a location (loc_rate[]): bit 15 set -> index into the
+ * per-step table of evaluated rate programs (rate_prog[]); clear -> index
+ * into inv_lit[].  Distinct rate programs are evaluated once per step per
+ * run instead of once per component. */
+#define CSMC_RATE_PROG_BIT 0x8000u
+#define CSMC_MAX_RATE_PROGS 64
 
 typedef struct {
     uint32_t loc_begin;  /* global index of the component's first location */

@@ -258,12 +258,17 @@ CSMC_HD float log2_pos(float x) {
     return f_add(static_cast<float>(e), lm);
 }
 
+// Reciprocal of an exponential rate as the delay formula uses it: the rate
+// rounded to float, then 1/rate correctly rounded.
+CSMC_HD float inv_rate(double rate) { return f_div(1.0f, d2f(rate)); }
+
 // Exponential delay: -log2(u) / rate, as the reference draws it
-// (simulation/simulation.cu:529-530: effective rate is rate * ln 2).
-CSMC_HD float exp_delay(uint32_t x, double rate) {
+// (simulation/simulation.cu:529-530: effective rate is rate * ln 2), computed
+// as -log2(u) * (1/rate) with the reciprocal above.
+CSMC_HD float exp_delay(uint32_t x, float inv) {
     const float u = uniform01(x);
     const float l = log2_pos(u);
-    return f_div(-l, d2f(rate));
+    return f_mul(-l, inv);
 }
 
 // Uniform delay on (0, max]: max * u in double, stored as float
@@ -379,9 +384,14 @@ CSMC_HD uint32_t delay_key(float d) {
 // component whose index has the smallest bit-reversal over log2 of the
 // padded width.  The kernels reduce on (key, bitrev(index)).
 CSMC_HD uint32_t bitrev_bits(uint32_t i, uint32_t bits) {
+    if (bits == 0) return 0;
+#ifdef __CUDA_ARCH__
+    return __brev(i) >> (32u - bits);
+#else
     uint32_t r = 0;
     for (uint32_t k = 0; k < bits; ++k) r |= ((i >> k) & 1u) << (bits - 1 - k);
     return r;
+#endif
 }
 
 CSMC_HD uint32_t ceil_log2(uint32_t n) {

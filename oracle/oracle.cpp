@@ -104,6 +104,7 @@ class Run {
             double r;
             switch (op) {
             case CSMC_OP_END: return top > 0 ? st[top - 1] : 0.0;
+            case CSMC_OP_HDR: continue;
             case CSMC_OP_PUSH_C: r = n_.konst[a]; break;
             case CSMC_OP_PUSH_V: r = static_cast<double>(vars_[a]); break;
             case CSMC_OP_ADD: r = v1 + v2; break;
@@ -193,7 +194,7 @@ class Run {
         }
         const uint32_t x = delay_word(seed_, run_, step_, c);
         if (bounded) return uniform_delay(x, max_delay);
-        return exp_delay(x, eval(L.rate));
+        return exp_delay(x, inv_rate(eval(L.rate)));
     }
 
     // simulation.cu:9-24 and 27-181.  en: enabled edge indices (ascending).

@@ -81,8 +81,9 @@ def main():
         for mode, query in (("var", lq), ("loc", lq)):
             out = subprocess.run([refdump, path, query, mode], capture_output=True, text=True)
             dump = out.stdout
-            with gzip.open(os.path.join(HERE, "frontend", f"{name}.{mode}.dump.gz"), "wt") as f:
-                f.write(dump)
+            with open(os.path.join(HERE, "frontend", f"{name}.{mode}.dump.gz"), "wb") as raw:
+                with gzip.GzipFile(fileobj=raw, mode="wb", mtime=0) as f:  # reproducible bytes
+                    f.write(dump.encode())
             entry = {"name": name, "mode": mode, "loc_query": query, "ref_status": out.returncode,
                      "generated": path.startswith(gen_dir)}
             if out.returncode == 0:
