@@ -54,11 +54,11 @@ class Result(ctypes.Structure):
         ("lanes_per_run", ctypes.c_int32),
         ("comps_per_lane", ctypes.c_int32),
         ("runs_per_cta", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("family", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class CsmcError(RuntimeError):
@@ -95,6 +95,8 @@ _SIGNATURES = {
                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
     "csmc_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                  ctypes.POINTER(ctypes.c_int32)]),
+    "csmc_set_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                     ctypes.c_int32]),
 }
 
 

@@ -129,6 +129,12 @@ class Network:
         check(lib().csmc_plan(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
+    def set_plan(self, family: int, lanes_per_run: int = 32, comps_per_lane: int = 1,
+                 threads_per_cta: int = 128) -> None:
+        """Selects the kernel family and launch shape (0: lane groups, 1: one
+        thread per run)."""
+        check(lib().csmc_set_plan(self._h, family, lanes_per_run, comps_per_lane, threads_per_cta))
+
     def run(self, query: Query, seed: int, n_runs: int, first_run: int = 0, flags=None, values=None, steps=None,
             stream: int | None = None) -> Result:
         """Simulates runs on the device; flags/values/steps are optional torch

@@ -34,9 +34,16 @@ struct csmc_net {
     uint64_t cap_runs = 0;
     double *d_partials = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // launch plan: family 0 = lane groups (lanes, comps_per_lane), 1 = one
+    // thread per run
+    int family = 1;
     int lanes = 0, comps_per_lane = 0, block = 256, grid = 0;
     size_t smem = 0;
     uint32_t state_stride = 0;
+    bool slots = false;
+    bool state_in_global = false;
+    uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
+    size_t state_bytes = 0;
 };
 
 namespace {
@@ -70,6 +77,67 @@ void choose_shape(uint32_t C, int &G, int &K) {
     G = 32;
     K = 2;
     while (static_cast<uint32_t>(G * K) < C) K <<= 1;
+}
+
+int max_smem_optin(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    return v;
+}
+
+// Fills the launch geometry of a plan; returns false when it cannot run.
+bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std::string &why) {
+    const csmc_net_header &h = n->h;
+    const size_t max_smem = static_cast<size_t>(max_smem_optin(n->device));
+    if (family == 0) {
+        if (!csmc::sim_supported(lanes, cpl) || static_cast<uint64_t>(lanes) * cpl < h.n_comps) {
+            why = "unsupported lane-group shape";
+            return false;
+        }
+        if (block <= 0 || block % 32 || block % lanes || block > 256) {
+            why = "lane-group plans use 32..256 threads per CTA";
+            return false;
+        }
+        // per-group run state: 48 bytes of scalars, the variables, then one
+        // inverse rate per rate program (evaluated once per step)
+        const uint32_t stride = static_cast<uint32_t>((48 + 4 * (h.n_vars + h.n_rate_prog) + 15) & ~15u);
+        const size_t smem = n->bytes + static_cast<size_t>(block / lanes) * stride;
+        if (smem > max_smem) {
+            why = "network and run state do not fit in shared memory";
+            return false;
+        }
+        n->family = 0;
+        n->lanes = lanes;
+        n->comps_per_lane = cpl;
+        n->block = block;
+        n->state_stride = stride;
+        n->smem = smem;
+        n->state_in_global = false;
+        return true;
+    }
+    if (block <= 0 || block % 32 || block > 128) {
+        why = "thread-per-run plans use 32..128 threads per CTA";
+        return false;
+    }
+    if (n->bytes > max_smem) {
+        why = "network does not fit in shared memory";
+        return false;
+    }
+    const size_t per_thread = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, n->slots);
+    const size_t slab = (per_thread * block + 15) & ~static_cast<size_t>(15);
+    n->family = 1;
+    n->lanes = 1;
+    n->comps_per_lane = static_cast<int>(h.n_comps);
+    n->block = block;
+    n->state_stride = static_cast<uint32_t>(slab);
+    if (n->bytes + slab <= max_smem) {
+        n->state_in_global = false;
+        n->smem = n->bytes + slab;
+    } else {
+        n->state_in_global = true;
+        n->smem = n->bytes;
+    }
+    return true;
 }
 
 const csmc_net_header *header_of(const void *blob, size_t bytes) {
@@ -136,6 +204,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     out->lanes_per_run = n->lanes;
     out->comps_per_lane = n->comps_per_lane;
     out->runs_per_cta = n->block / n->lanes;
+    out->family = n->family;
     if (n_runs == 0) return CSMC_OK;
     CK(cudaSetDevice(n->device), "cudaSetDevice");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -166,18 +235,34 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     p.final_state = final_state;
     p.scratch = n->d_scratch;
     int ctas = 0;
-    int rc = csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas);
+    int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
+                            : csmc::serial_max_active_ctas(verify, n->slots, n->block, n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network (shared memory)");
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device), "cudaDeviceGetAttribute");
-    const uint64_t groups_per_cta = static_cast<uint64_t>(n->block / n->lanes);
+    const uint64_t runs_per_cta = static_cast<uint64_t>(n->block / n->lanes);
     uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(ctas);
-    const uint64_t needed = (n_runs + groups_per_cta - 1) / groups_per_cta;
+    const uint64_t needed = (n_runs + runs_per_cta - 1) / runs_per_cta;
     if (grid > needed) grid = needed;
     n->grid = static_cast<int>(grid);
+    p.state_global = nullptr;
+    if (n->family == 1 && n->state_in_global) {
+        const size_t need = grid * static_cast<size_t>(n->state_stride);
+        if (need > n->state_bytes) {
+            cudaFree(n->d_state);
+            n->d_state = nullptr;
+            n->state_bytes = 0;
+            CK(cudaMalloc(&n->d_state, need), "cudaMalloc(run state)");
+            n->state_bytes = need;
+        }
+        p.state_global = n->d_state;
+    }
+    p.state_stride = n->state_stride;
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
-    rc = csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block, n->smem, st);
+    rc = n->family == 0
+             ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block, n->smem, st)
+             : csmc::serial_launch(verify, n->slots, p, static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
     if (need_values) reduce_values<<<kReduceBlocks, 256, 0, st>>>(values, n_runs, n->d_partials);
@@ -320,17 +405,19 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     CK(cudaGetDevice(&n->device), "cudaGetDevice");
     n->h = *h;
     n->bytes = (h->total_bytes + 15u) & ~15u;
-    choose_shape(h->n_comps, n->lanes, n->comps_per_lane);
-    if (!csmc::sim_supported(n->lanes, n->comps_per_lane))
-        return fail(CSMC_ERR_LIMIT, "networks with more than 1024 components are not supported");
-    // per-group run state: 48 bytes of scalars, the variables, then one
-    // inverse rate per rate program (evaluated once per step)
-    n->state_stride = static_cast<uint32_t>((48 + 4 * (h->n_vars + h->n_rate_prog) + 15) & ~15u);
-    n->smem = n->bytes + static_cast<size_t>(n->block / n->lanes) * n->state_stride;
-    int max_smem = 0;
-    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device), "attribute");
-    if (n->smem > static_cast<size_t>(max_smem))
-        return fail(CSMC_ERR_LIMIT, "network (" + std::to_string(n->bytes) + " bytes) does not fit in shared memory");
+    n->slots = h->max_edges_per_loc >= 2;
+    // default plan: one thread per run when the run state of a 128-thread
+    // CTA fits next to the network in shared memory, lane groups otherwise
+    std::string why;
+    int G = 0, K = 0;
+    choose_shape(h->n_comps, G, K);
+    const size_t per_thread = csmc::serial_state_bytes_per_thread(h->n_comps, h->n_vars, h->n_rate_prog, n->slots);
+    const bool serial_fits = n->bytes + 128 * per_thread <= static_cast<size_t>(max_smem_optin(n->device));
+    bool ok = false;
+    if (serial_fits) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
+    if (!ok) ok = configure_plan(n.get(), 0, G, K, 256, why);
+    if (!ok) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
+    if (!ok) return fail(CSMC_ERR_LIMIT, "no launch plan for this network: " + why);
     CK(cudaMalloc(&n->d_blob, n->bytes), "cudaMalloc(network)");
     CK(cudaMemset(n->d_blob, 0, n->bytes), "cudaMemset");
     CK(cudaMemcpy(n->d_blob, blob, h->total_bytes, cudaMemcpyHostToDevice), "cudaMemcpy(network)");
@@ -349,9 +436,28 @@ void csmc_net_free(csmc_net *n) {
     cudaFree(n->d_flags);
     cudaFree(n->d_values);
     cudaFree(n->d_partials);
+    cudaFree(n->d_state);
     if (n->ev0) cudaEventDestroy(n->ev0);
     if (n->ev1) cudaEventDestroy(n->ev1);
     delete n;
+}
+
+int csmc_set_plan(csmc_net *n, int32_t family, int32_t lanes_per_run, int32_t comps_per_lane,
+                  int32_t threads_per_cta) {
+    if (!n) return fail(CSMC_ERR_ARG, "null argument");
+    const csmc_net saved = *n;
+    std::string why;
+    if (!configure_plan(n, family, lanes_per_run, comps_per_lane, threads_per_cta, why)) {
+        n->family = saved.family;
+        n->lanes = saved.lanes;
+        n->comps_per_lane = saved.comps_per_lane;
+        n->block = saved.block;
+        n->smem = saved.smem;
+        n->state_stride = saved.state_stride;
+        n->state_in_global = saved.state_in_global;
+        return fail(CSMC_ERR_ARG, "plan rejected: " + why);
+    }
+    return CSMC_OK;
 }
 
 int csmc_plan(const csmc_net *n, int32_t *lanes, int32_t *cpl, int32_t *rpc) {

@@ -623,6 +623,13 @@ class Packer {
                     h.n_channels_max = std::max<uint32_t>(h.n_channels_max, static_cast<uint32_t>(std::abs(e.channel)));
                 }
                 pl.n_recv = static_cast<uint8_t>(nrecv);
+                for (const DevEdge &e : L.edges) {
+                    if (e.channel >= 0) continue;
+                    const uint32_t ch = static_cast<uint32_t>(-e.channel);
+                    if (ch < 32) h.recv_chan_lo |= 1u << ch;
+                    else if (ch < 63) h.recv_chan_hi |= 1u << (ch - 32);
+                    else h.recv_chan_hi |= 1u << 31;
+                }
                 locs_.push_back(pl);
                 // edges are appended after all locations of the component so
                 // that a location's edges stay contiguous
@@ -633,11 +640,15 @@ class Packer {
             }
         }
         if (nv > 65535) fail("too many variables");
+        std::vector<uint16_t> clocks;
         for (uint32_t i = 0; i < nv; ++i) {
             csmc_var v;
             v.init = static_cast<float>(m_.var_init[i]);
             v.kind = m_.var_kind_clock[i] ? 1u : 0u;
-            if (v.kind) ++h.n_clocks;
+            if (v.kind) {
+                ++h.n_clocks;
+                clocks.push_back(static_cast<uint16_t>(i));
+            }
             vars_.push_back(v);
         }
         // rate slots: literal rates pre-inverted on the host, other rate
@@ -703,6 +714,7 @@ class Packer {
         h.off_loc_rate = section(loc_rate.data(), loc_rate.size() * sizeof(uint16_t));
         h.off_inv_lit = section(inv_lit.data(), inv_lit.size() * sizeof(float));
         h.off_rate_prog = section(rate_prog.data(), rate_prog.size() * sizeof(uint32_t));
+        h.off_clock = section(clocks.data(), clocks.size() * sizeof(uint16_t));
         while (out.size() % 16) out.push_back(0);
         h.total_bytes = static_cast<uint32_t>(out.size());
         std::memcpy(out.data(), &h, sizeof h);

@@ -81,7 +81,10 @@ typedef struct {
     uint32_t off_loc_rate;   /* uint16 per location: rate slot */
     uint32_t off_inv_lit;    /* float per literal rate: 1/rate (inv_rate of csmc_numeric.h) */
     uint32_t off_rate_prog;  /* uint32 expression handle per rate program */
-    uint32_t reserved[6];
+    uint32_t recv_chan_lo;   /* bit c: some location can receive on channel c (c < 32) */
+    uint32_t recv_chan_hi;   /* channels 32..63; bit 31 also stands for every channel >= 63 */
+    uint32_t off_clock;      /* uint16 id per clock variable (n_clocks entries) */
+    uint32_t reserved[3];
 } csmc_net_header; /* 160 bytes */
 
 /* Header flags. */

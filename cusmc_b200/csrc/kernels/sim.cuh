@@ -48,14 +48,28 @@ struct SimParams {
     uint64_t *digests;         // verification outputs (may be null)
     uint32_t *final_state;
     unsigned long long *scratch;  // [0] work counter [1] hits [2] steps [3] capped [4] errors
+    uint8_t *state_global;        // thread-per-run kernel: per-CTA state slabs in global memory
+                                  // (null: state in shared memory after the network)
 };
 
 #define CSMC_SCRATCH_WORDS 8
 
-// Launch entry points (defined in sim_kernel.cu).
+// Launch entry points (sim_dispatch.cu).  Lane-group kernel family:
 int sim_launch(int lanes_per_run, int comps_per_lane, bool verify, const SimParams &p, int grid, int block,
                size_t smem, void *stream);
 int sim_max_active_ctas(int lanes_per_run, int comps_per_lane, bool verify, int block, size_t smem, int *ctas);
 bool sim_supported(int lanes_per_run, int comps_per_lane);
+// Thread-per-run kernel family (slots: the network has locations with
+// several edges, so enabled-edge slot masks are kept):
+int serial_launch(bool verify, bool slots, const SimParams &p, int grid, int block, size_t smem, void *stream);
+int serial_max_active_ctas(bool verify, bool slots, int block, size_t smem, int *ctas);
+
+// Bytes of thread-per-run state per thread for a network.
+inline size_t serial_state_bytes_per_thread(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots) {
+    size_t b = 4u * (2u * n_vars + n_rate_prog);  // variables, rate table, receiver snapshot
+    b += (2u * n_comps + 3u) & ~3u;               // locations (uint16)
+    if (slots) b += 4u * n_comps;                 // enabled-edge slot masks
+    return b;
+}
 
 }  // namespace csmc

@@ -10,6 +10,24 @@ template <int G, int K, bool VERIFY>
 int launch_one(const SimParams &p, int grid, int block, size_t smem, void *stream);
 template <int G, int K, bool VERIFY>
 int occupancy_one(int block, size_t smem, int *ctas);
+template <bool VERIFY, bool SLOTS>
+int serial_launch_one(const SimParams &p, int grid, int block, size_t smem, void *stream);
+template <bool VERIFY, bool SLOTS>
+int serial_occupancy_one(int block, size_t smem, int *ctas);
+
+int serial_launch(bool verify, bool slots, const SimParams &p, int grid, int block, size_t smem, void *stream) {
+    if (verify) return slots ? serial_launch_one<true, true>(p, grid, block, smem, stream)
+                             : serial_launch_one<true, false>(p, grid, block, smem, stream);
+    return slots ? serial_launch_one<false, true>(p, grid, block, smem, stream)
+                 : serial_launch_one<false, false>(p, grid, block, smem, stream);
+}
+
+int serial_max_active_ctas(bool verify, bool slots, int block, size_t smem, int *ctas) {
+    if (verify) return slots ? serial_occupancy_one<true, true>(block, smem, ctas)
+                             : serial_occupancy_one<true, false>(block, smem, ctas);
+    return slots ? serial_occupancy_one<false, true>(block, smem, ctas)
+                 : serial_occupancy_one<false, false>(block, smem, ctas);
+}
 
 #define CSMC_SHAPES(X) X(1, 1) X(2, 1) X(4, 1) X(8, 1) X(16, 1) X(32, 1) X(32, 2) X(32, 4) X(32, 8) X(32, 16) X(32, 32)
 

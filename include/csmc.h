@@ -69,10 +69,10 @@ typedef struct {
     double sum_sq;       /* variable query: sum of squares */
     double estimate;     /* location: hits/runs; variable: mean or fraction */
     double kernel_ms;    /* device time of the simulation kernel(s) */
-    int32_t lanes_per_run;
-    int32_t comps_per_lane;
-    int32_t runs_per_cta;
-    int32_t reserved;
+    int32_t lanes_per_run;  /* launch plan used: lanes per run (1: one thread per run) */
+    int32_t comps_per_lane; /* components per lane */
+    int32_t runs_per_cta;   /* runs in flight per CTA */
+    int32_t family;         /* 0 lane-group kernel, 1 thread-per-run kernel */
 } csmc_result;
 
 /* Thread-local message of the last failure on this thread. */
@@ -133,6 +133,13 @@ int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int thr
 /* Sizes a launch would use for this network: lanes per run, components per
  * lane, runs per CTA. */
 int csmc_plan(const csmc_net *net, int32_t *lanes_per_run, int32_t *comps_per_lane, int32_t *runs_per_cta);
+
+/* Overrides the launch plan of a network handle (used by the autotuner):
+ * family 0 = lane groups of lanes_per_run lanes (power of two <= 32) with
+ * comps_per_lane components each; family 1 = one thread per run (lanes and
+ * comps_per_lane are ignored).  threads_per_cta: CTA size. */
+int csmc_set_plan(csmc_net *net, int32_t family, int32_t lanes_per_run, int32_t comps_per_lane,
+                  int32_t threads_per_cta);
 
 #ifdef __cplusplus
 }

@@ -20,10 +20,29 @@ from cusmc_b200 import api, netgen
 pytestmark = pytest.mark.gpu
 
 
-def _compare(blob, query, seed, n_runs, first_run=0):
+def _lane_shape(n_comps):
+    if n_comps <= 32:
+        g = 1
+        while g < n_comps:
+            g *= 2
+        return g, 1
+    k = 2
+    while 32 * k < n_comps:
+        k *= 2
+    return 32, k
+
+
+def _compare(blob, query, seed, n_runs, first_run=0, family=None):
+    """family None: the library's default plan; 0: lane groups; 1: one
+    thread per run."""
     import oracle
     net = api.Network(blob)
     try:
+        if family == 0:
+            g, k = _lane_shape(net.info["n_comps"])
+            net.set_plan(0, g, k, 256)
+        elif family == 1:
+            net.set_plan(1, 1, 1, 128)
         r_dev, dev = net.run_verify(query, seed, n_runs, first_run)
     finally:
         net.close()
@@ -35,6 +54,8 @@ def _compare(blob, query, seed, n_runs, first_run=0):
             raise AssertionError(f"{key} differs on {len(bad)} of {n_runs} runs, first run {bad[0] + first_run}")
     assert np.array_equal(dev["values"].view(np.uint64), cpu["values"].view(np.uint64))
     assert r_dev.hits == r_cpu.hits and r_dev.steps == r_cpu.steps and r_dev.capped == r_cpu.capped
+    if family is not None:
+        assert r_dev.family == family
     return r_dev, r_cpu
 
 
@@ -50,8 +71,9 @@ def _fixture_nets():
 FIXTURE_CASES = [(m["name"], m["mode"]) for m in _fixture_nets() if m["name"] != "CSMA_100"]
 
 
+@pytest.mark.parametrize("family", [0, 1])
 @pytest.mark.parametrize("name,mode", FIXTURE_CASES)
-def test_reference_fixtures(name, mode):
+def test_reference_fixtures(name, mode, family):
     with open(os.path.join(GOLDEN, "nets", f"{name}.{mode}.blob"), "rb") as f:
         blob = f.read()
     info = api.blob_info(blob)
@@ -65,7 +87,7 @@ def test_reference_fixtures(name, mode):
         q = api.variable_query(var_id=min(1, info["n_vars"] - 1), horizon=100, threshold=0, is_max=True,
                                max_steps=cap)
     runs = 128 if info["n_comps"] >= 100 else 512
-    _compare(blob, q, seed=1235, n_runs=runs)
+    _compare(blob, q, seed=1235, n_runs=runs, family=family)
 
 
 def _blob(w, loc=False):
@@ -79,27 +101,30 @@ def _blob(w, loc=False):
         os.unlink(path)
 
 
-def test_epidemic_1000_runs():
+@pytest.mark.parametrize("family", [0, 1])
+def test_epidemic_1000_runs(family):
     w = netgen.epidemic()
     blob = _blob(w)
     q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
-    _compare(blob, q, seed=2024, n_runs=1000)
+    _compare(blob, q, seed=2024, n_runs=1000, family=family)
 
 
+@pytest.mark.parametrize("family", [0, 1])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
-def test_random_networks(seed):
+def test_random_networks(seed, family):
     w = netgen.random_network(seed)
     blob = _blob(w)
     q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
-    _compare(blob, q, seed=7 + seed, n_runs=2000)
+    _compare(blob, q, seed=7 + seed, n_runs=2000, family=family)
 
 
+@pytest.mark.parametrize("family", [0, 1])
 @pytest.mark.parametrize("n", [8, 32])
-def test_mutex(n):
+def test_mutex(n, family):
     w = netgen.mutex(n)
     blob = _blob(w)
     q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
-    _compare(blob, q, seed=99, n_runs=500)
+    _compare(blob, q, seed=99, n_runs=500, family=family)
 
 
 def test_first_run_offset_is_the_same_stream():
