@@ -342,6 +342,11 @@ void write_timing_csv(const std::string &xml_path, int mc, int sims, double time
 
 }  // namespace
 
+namespace csmc {
+// Lets other translation units of the library report through csmc_last_error().
+void set_last_error(const std::string &m) { g_err = m; }
+}  // namespace csmc
+
 extern "C" {
 
 const char *csmc_last_error(void) { return g_err.c_str(); }

@@ -141,6 +141,39 @@ int csmc_plan(const csmc_net *net, int32_t *lanes_per_run, int32_t *comps_per_la
 int csmc_set_plan(csmc_net *net, int32_t family, int32_t lanes_per_run, int32_t comps_per_lane,
                   int32_t threads_per_cta);
 
+/* Scratch bytes per device behind csmc_run_noalloc (held from the first
+ * call on a device until the process exits). */
+#define CSMC_NOALLOC_SCRATCH_BYTES (2u * 1024u * 1024u)
+
+/* csmc_run_noalloc — has no counterpart in the reference.
+ *
+ * The thread-per-run simulation of csmc_run for callers that cannot let a
+ * library allocate device memory: hosts that reserve all device memory
+ * themselves at start-up and forbid later cudaMalloc/cudaFree, loops in which
+ * cudaMalloc's implicit device synchronisation is not acceptable, or
+ * frameworks whose own allocator must own every buffer.  The caller passes
+ * the packed network twice — blob_host (host memory, for the launch plan) and
+ * blob_device (the same bytes in device memory, 16-byte aligned) — and the
+ * device output buffers; flags/values/steps as in csmc_run, except that
+ * values is required for variable queries.  Nothing is allocated: the
+ * kernel's scratch (work and result counters, partial sums, and run-state
+ * slabs when a network's run state does not fit in shared memory) is a
+ * file-scope device array of CSMC_NOALLOC_SCRATCH_BYTES bytes per device.
+ * Networks whose run state needs more than that are rejected with
+ * CSMC_ERR_LIMIT; fewer CTAs are launched when the slabs would not all fit.
+ *
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Every call on a device shares the one array
+ * and overwrites what the previous call left there (the counters are cleared
+ * at the start of each call): calls whose work overlaps on the GPU, from
+ * several host threads or on several streams, race and return wrong counts.
+ * kernel_ms is not measured (0).  Results, run for run, are those of
+ * csmc_run with the thread-per-run plan. */
+int csmc_run_noalloc(const void *blob_host, const void *blob_device, size_t bytes, const csmc_query *q,
+                     uint64_t seed, uint64_t first_run, uint64_t n_runs, uint8_t *flags, double *values,
+                     uint32_t *steps, csmc_result *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
