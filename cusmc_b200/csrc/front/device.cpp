@@ -684,6 +684,25 @@ class Packer {
             h.n_inv_lit = static_cast<uint32_t>(inv_lit.size());
             if (h.n_rate_prog <= CSMC_MAX_RATE_PROGS) h.flags |= CSMC_NET_RATE_TABLE;
         }
+        std::vector<uint64_t> loc_desc;
+        for (size_t i = 0; i < locs_.size(); ++i) {
+            const csmc_loc &pl = locs_[i];
+            uint32_t flags = 0, lo = 0;
+            if (pl.type > 1) flags |= CSMC_DESC_ZERO;
+            if (pl.n_inv) flags |= CSMC_DESC_INV;
+            const uint16_t slot = loc_rate[i];
+            if (slot & CSMC_RATE_PROG_BIT) {
+                if (h.flags & CSMC_NET_RATE_TABLE) {
+                    flags |= CSMC_DESC_PROG;
+                    lo = slot & ~CSMC_RATE_PROG_BIT;
+                } else {
+                    flags |= CSMC_DESC_EVAL;
+                }
+            } else {
+                std::memcpy(&lo, &inv_lit[slot], 4);
+            }
+            loc_desc.push_back(static_cast<uint64_t>(lo) | (static_cast<uint64_t>(flags) << 32));
+        }
         h.magic = CSMC_NET_MAGIC;
         h.version = CSMC_NET_VERSION;
         h.header_bytes = sizeof(csmc_net_header);
@@ -715,6 +734,7 @@ class Packer {
         h.off_inv_lit = section(inv_lit.data(), inv_lit.size() * sizeof(float));
         h.off_rate_prog = section(rate_prog.data(), rate_prog.size() * sizeof(uint32_t));
         h.off_clock = section(clocks.data(), clocks.size() * sizeof(uint16_t));
+        h.off_loc_desc = section(loc_desc.data(), loc_desc.size() * sizeof(uint64_t));
         while (out.size() % 16) out.push_back(0);
         h.total_bytes = static_cast<uint32_t>(out.size());
         std::memcpy(out.data(), &h, sizeof h);

@@ -84,7 +84,8 @@ typedef struct {
     uint32_t recv_chan_lo;   /* bit c: some location can receive on channel c (c < 32) */
     uint32_t recv_chan_hi;   /* channels 32..63; bit 31 also stands for every channel >= 63 */
     uint32_t off_clock;      /* uint16 id per clock variable (n_clocks entries) */
-    uint32_t reserved[3];
+    uint32_t off_loc_desc;   /* uint64 delay descriptor per location (CSMC_DESC_*) */
+    uint32_t reserved[2];
 } csmc_net_header; /* 160 bytes */
 
 /* Header flags. */
@@ -96,6 +97,15 @@ typedef struct {
  * run instead of once per component. */
 #define CSMC_RATE_PROG_BIT 0x8000u
 #define CSMC_MAX_RATE_PROGS 64
+
+/* Delay descriptor of a location (loc_desc[]): everything the per-component
+ * delay needs in one 8-byte word.  Low 32 bits: the float 1/rate of a
+ * literal rate, or the rate-table slot of a rate program (DESC_PROG).  High
+ * 32 bits: flags. */
+#define CSMC_DESC_PROG (1u << 0)  /* low word is a rate-table slot */
+#define CSMC_DESC_ZERO (1u << 1)  /* branch / urgent / committed: delay 0 */
+#define CSMC_DESC_INV (1u << 2)   /* has delay-bounding invariants */
+#define CSMC_DESC_EVAL (1u << 3)  /* rate evaluated per component (no table) */
 
 typedef struct {
     uint32_t loc_begin;  /* global index of the component's first location */

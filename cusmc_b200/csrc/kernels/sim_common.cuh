@@ -28,6 +28,7 @@ struct Net {
     const float *inv_lit;
     const uint32_t *rate_prog;
     const uint16_t *clock;
+    const uint64_t *loc_desc;
     uint32_t n_comps, n_vars, n_rate_prog, flags, n_clocks, recv_lo, recv_hi;
 };
 
@@ -46,6 +47,7 @@ static __device__ __forceinline__ Net net_view(const uint8_t *base) {
     n.inv_lit = reinterpret_cast<const float *>(base + h->off_inv_lit);
     n.rate_prog = reinterpret_cast<const uint32_t *>(base + h->off_rate_prog);
     n.clock = reinterpret_cast<const uint16_t *>(base + h->off_clock);
+    n.loc_desc = reinterpret_cast<const uint64_t *>(base + h->off_loc_desc);
     n.n_comps = h->n_comps;
     n.n_vars = h->n_vars;
     n.n_rate_prog = h->n_rate_prog;
@@ -138,13 +140,9 @@ static __device__ __noinline__ double eval_stack(const Net &n, VarView vars, uin
     }
 }
 
-// Any expression handle.  Literals and variables directly; programs that
-// only ever read the two top entries (header flag WINDOW) with two
-// registers; the rest on the stack machine.
-static __device__ __forceinline__ double eval(const Net &n, VarView vars, uint32_t h) {
-    const uint32_t tag = CSMC_H_TAG(h), p = CSMC_H_PAYLOAD(h);
-    if (tag == CSMC_H_LIT) return n.konst[p];
-    if (tag == CSMC_H_VAR) return static_cast<double>(vars[p]);
+// Programs that only ever read the two top entries (header flag WINDOW)
+// run on two registers; the rest on the stack machine.
+static __device__ __noinline__ double eval_prog(const Net &n, VarView vars, uint32_t p) {
     if (!(CSMC_INS_A(n.code[p]) & CSMC_PROG_WINDOW)) return eval_stack(n, vars, p);
     double a = 0.0, b = 0.0;
     for (uint32_t ip = p + 1;; ++ip) {
@@ -158,6 +156,14 @@ static __device__ __forceinline__ double eval(const Net &n, VarView vars, uint32
         a = b;
         b = r;
     }
+}
+
+// Any expression handle: literals and variables inline, programs out of line.
+static __device__ __forceinline__ double eval(const Net &n, VarView vars, uint32_t h) {
+    const uint32_t tag = CSMC_H_TAG(h), p = CSMC_H_PAYLOAD(h);
+    if (tag == CSMC_H_LIT) return n.konst[p];
+    if (tag == CSMC_H_VAR) return static_cast<double>(vars[p]);
+    return eval_prog(n, vars, p);
 }
 
 // simulation.cu:184-266

@@ -21,6 +21,12 @@
 namespace csmc {
 namespace detail {
 
+// Delay of a component whose location is invariant-bounded, or whose rate
+// is evaluated per component (uncommon; out of line).
+static __device__ __noinline__ float slow_delay(const Net &n, VarView vars, VarView rates, uint32_t li, uint32_t x) {
+    return comp_delay(n, vars, rates, li, x);
+}
+
 #ifndef CSMC_SERIAL_MIN_CTAS_PER_SM
 #define CSMC_SERIAL_MIN_CTAS_PER_SM 1
 #endif
@@ -166,7 +172,19 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             for (uint32_t k = 0; k < 4; ++k) {
                 const uint32_t cc = c + k;
                 if (cc < C) {
-                    const float d = comp_delay(n, vars, rates, locs[cc * T], word_of(blk, k));
+                    // fast path from the location's delay descriptor: the
+                    // exponential delay with the literal 1/rate or the
+                    // step's evaluated rate; zero-delay types and bounded
+                    // locations take the general path
+                    const uint32_t li = locs[cc * T];
+                    const uint64_t dsc = n.loc_desc[li];
+                    const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
+                    const uint32_t x = word_of(blk, k);
+                    float inv = __uint_as_float(lo);
+                    if (fl & CSMC_DESC_PROG) inv = rates[lo];
+                    float d = exp_delay(x, inv);
+                    if (fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL))
+                        d = (fl & CSMC_DESC_ZERO) ? 0.0f : slow_delay(n, vars, rates, li, x);
                     const unsigned long long key =
                         (static_cast<unsigned long long>(delay_key(d)) << 32) | bitrev_bits(cc, bits);
                     if (key < best) {

@@ -94,6 +94,19 @@ def main():
                         f.write(blob)
             manifest["models"].append(entry)
             print(name, mode, out.returncode, len(dump))
+    # packed networks of the reference-estimate cases (make_ref_estimates.py),
+    # compiled with exactly the query each reference run used
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("refest", os.path.join(HERE, "make_ref_estimates.py"))
+    refest = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(refest)
+    for name, src, qargs, _sims, _seed in refest.CASES:
+        if src.startswith("gen:"):
+            continue
+        path = os.path.join(args.ref, "xml_files", src)
+        blob = api.compile_model(path, qargs[5], qargs[2] == "-1")
+        with open(os.path.join(HERE, "nets", f"refest_{name}.blob"), "wb") as f:
+            f.write(blob)
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
         json.dump(manifest, f, indent=1)
 
