@@ -41,6 +41,7 @@ struct csmc_net {
     size_t smem = 0;
     uint32_t state_stride = 0;
     bool slots = false;
+    bool loc8 = false;  // every automaton has at most 256 locations
     bool state_in_global = false;
     uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
     size_t state_bytes = 0;
@@ -123,7 +124,7 @@ bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std:
         why = "network does not fit in shared memory";
         return false;
     }
-    const size_t per_thread = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, n->slots);
+    const size_t per_thread = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, n->slots, n->loc8);
     const size_t slab = (per_thread * block + 15) & ~static_cast<size_t>(15);
     n->family = 1;
     n->lanes = 1;
@@ -216,6 +217,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     }
     CK(cudaMemsetAsync(n->d_scratch, 0, CSMC_SCRATCH_WORDS * sizeof(unsigned long long), st), "cudaMemsetAsync");
     csmc::SimParams p{};
+    p.net = csmc::layout_of(n->h);
     p.blob = n->d_blob;
     p.blob_bytes = n->bytes;
     p.state_stride = n->state_stride;
@@ -236,7 +238,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     p.scratch = n->d_scratch;
     int ctas = 0;
     int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
-                            : csmc::serial_max_active_ctas(verify, n->slots, n->block, n->smem, &ctas);
+                            : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->block, n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network (shared memory)");
     int sms = 0;
@@ -262,7 +264,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
     rc = n->family == 0
              ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block, n->smem, st)
-             : csmc::serial_launch(verify, n->slots, p, static_cast<int>(grid), n->block, n->smem, st);
+             : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, p, static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
     if (need_values) reduce_values<<<kReduceBlocks, 256, 0, st>>>(values, n_runs, n->d_partials);
@@ -411,12 +413,13 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     n->h = *h;
     n->bytes = (h->total_bytes + 15u) & ~15u;
     n->slots = h->max_edges_per_loc >= 2;
+    n->loc8 = h->max_locs_per_comp <= 256;
     // default plan: one thread per run when the run state of a 128-thread
     // CTA fits next to the network in shared memory, lane groups otherwise
     std::string why;
     int G = 0, K = 0;
     choose_shape(h->n_comps, G, K);
-    const size_t per_thread = csmc::serial_state_bytes_per_thread(h->n_comps, h->n_vars, h->n_rate_prog, n->slots);
+    const size_t per_thread = csmc::serial_state_bytes_per_thread(h->n_comps, h->n_vars, h->n_rate_prog, n->slots, n->loc8);
     const bool serial_fits = n->bytes + 128 * per_thread <= static_cast<size_t>(max_smem_optin(n->device));
     bool ok = false;
     if (serial_fits) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);

@@ -27,7 +27,23 @@
 
 namespace csmc {
 
+// Section offsets and counts of the packed network (copied from its header
+// by the host, so kernels read them from the parameter bank).
+struct NetLayout {
+    uint32_t off_comp, off_loc, off_edge, off_guard, off_update, off_var, off_const, off_code;
+    uint32_t off_loc_rate, off_inv_lit, off_rate_prog, off_clock, off_loc_desc;
+    uint32_t n_comps, n_vars, n_rate_prog, flags, n_clocks, recv_lo, recv_hi;
+};
+
+inline NetLayout layout_of(const csmc_net_header &h) {
+    return NetLayout{h.off_comp,     h.off_loc,     h.off_edge,      h.off_guard,    h.off_update,
+                     h.off_var,      h.off_const,   h.off_code,      h.off_loc_rate, h.off_inv_lit,
+                     h.off_rate_prog, h.off_clock,  h.off_loc_desc,  h.n_comps,      h.n_vars,
+                     h.n_rate_prog,  h.flags,       h.n_clocks,      h.recv_chan_lo, h.recv_chan_hi};
+}
+
 struct SimParams {
+    NetLayout net;             // layout of the network staged at the start of shared memory
     const uint8_t *blob;       // packed network in global memory
     uint32_t blob_bytes;       // bytes to stage (multiple of 16)
     uint32_t state_stride;     // bytes of per-group run state in shared memory (multiple of 16)
@@ -61,14 +77,18 @@ int sim_max_active_ctas(int lanes_per_run, int comps_per_lane, bool verify, int 
 bool sim_supported(int lanes_per_run, int comps_per_lane);
 // Thread-per-run kernel family (slots: the network has locations with
 // several edges, so enabled-edge slot masks are kept):
-int serial_launch(bool verify, bool slots, const SimParams &p, int grid, int block, size_t smem, void *stream);
-int serial_max_active_ctas(bool verify, bool slots, int block, size_t smem, int *ctas);
+// loc8: locations kept as 8-bit local indices (every automaton has at most
+// 256 locations); gstate: run state in global slabs instead of shared memory.
+int serial_launch(bool verify, bool slots, bool loc8, bool gstate, const SimParams &p, int grid, int block,
+                  size_t smem, void *stream);
+int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, int block, size_t smem, int *ctas);
 
 // Bytes of thread-per-run state per thread for a network.
-inline size_t serial_state_bytes_per_thread(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots) {
-    size_t b = 4u * (2u * n_vars + n_rate_prog);  // variables, rate table, receiver snapshot
-    b += (2u * n_comps + 3u) & ~3u;               // locations (uint16)
-    if (slots) b += 4u * n_comps;                 // enabled-edge slot masks
+inline size_t serial_state_bytes_per_thread(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots,
+                                            bool loc8) {
+    size_t b = 4u * (2u * n_vars + n_rate_prog);        // variables, rate table, receiver snapshot
+    b += loc8 ? ((n_comps + 3u) & ~3u) : ((2u * n_comps + 3u) & ~3u);  // locations
+    if (slots) b += 4u * n_comps;                       // enabled-edge slot masks
     return b;
 }
 

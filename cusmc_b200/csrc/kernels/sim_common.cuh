@@ -58,6 +58,32 @@ static __device__ __forceinline__ Net net_view(const uint8_t *base) {
     return n;
 }
 
+// The same view with offsets and counts taken from the kernel parameters.
+static __device__ __forceinline__ Net net_view(const uint8_t *base, const NetLayout &l) {
+    Net n;
+    n.comp = reinterpret_cast<const csmc_comp *>(base + l.off_comp);
+    n.loc = reinterpret_cast<const csmc_loc *>(base + l.off_loc);
+    n.edge = reinterpret_cast<const csmc_edge *>(base + l.off_edge);
+    n.guard = reinterpret_cast<const csmc_guard *>(base + l.off_guard);
+    n.upd = reinterpret_cast<const csmc_update *>(base + l.off_update);
+    n.var = reinterpret_cast<const csmc_var *>(base + l.off_var);
+    n.konst = reinterpret_cast<const double *>(base + l.off_const);
+    n.code = reinterpret_cast<const uint64_t *>(base + l.off_code);
+    n.loc_rate = reinterpret_cast<const uint16_t *>(base + l.off_loc_rate);
+    n.inv_lit = reinterpret_cast<const float *>(base + l.off_inv_lit);
+    n.rate_prog = reinterpret_cast<const uint32_t *>(base + l.off_rate_prog);
+    n.clock = reinterpret_cast<const uint16_t *>(base + l.off_clock);
+    n.loc_desc = reinterpret_cast<const uint64_t *>(base + l.off_loc_desc);
+    n.n_comps = l.n_comps;
+    n.n_vars = l.n_vars;
+    n.n_rate_prog = l.n_rate_prog;
+    n.flags = l.flags;
+    n.n_clocks = l.n_clocks;
+    n.recv_lo = l.recv_lo;
+    n.recv_hi = l.recv_hi;
+    return n;
+}
+
 // Whether any location can receive on channel ch (> 0).
 static __device__ __forceinline__ bool has_receivers(const Net &n, int ch) {
     if (ch < 32) return (n.recv_lo >> ch) & 1u;

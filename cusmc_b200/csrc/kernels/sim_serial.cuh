@@ -9,8 +9,15 @@
 // warp.  Per-run state lives in interleaved arrays (element i of thread t at
 // [i * threads + t], conflict-free in shared memory): variables, the
 // evaluated rate table, a snapshot of the variables for broadcast receivers,
-// component locations (uint16 global location index) and, when some location
-// has several edges, the enabled-edge slot masks.
+// component locations and, when some location has several edges, the
+// enabled-edge slot masks.
+//
+// Template options: SLOTS keeps the slot masks; LOC8 stores locations as
+// 8-bit local indices (automata of at most 256 locations), otherwise as
+// 16-bit global indices; GSTATE puts the state in per-CTA global slabs when
+// it does not fit in shared memory.  The network layout comes from the
+// kernel parameters, so pointers into the staged network are rebuilt from
+// constants instead of occupying registers.
 //
 // The component order, the race tie-break, the Philox draws and every
 // arithmetic step are those of the lane-group kernel and the CPU oracle
@@ -28,37 +35,47 @@ static __device__ __noinline__ float slow_delay(const Net &n, VarView vars, VarV
 }
 
 #ifndef CSMC_SERIAL_MIN_CTAS_PER_SM
-#define CSMC_SERIAL_MIN_CTAS_PER_SM 1
+#define CSMC_SERIAL_MIN_CTAS_PER_SM 5
 #endif
 
-template <bool VERIFY, bool SLOTS>
+template <bool LOC8>
+struct LocStore {
+    using T = uint16_t;  // global location index
+};
+template <>
+struct LocStore<true> {
+    using T = uint8_t;   // local location index
+};
+
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
 __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kernel(const SimParams p) {
+    using LocT = typename LocStore<LOC8>::T;
     extern __shared__ __align__(16) uint8_t smem[];
     stage_network(smem, p.blob, p.blob_bytes);
     __syncthreads();
-    const Net n = net_view(smem);
-    const uint32_t C = n.n_comps, V = n.n_vars, P = n.n_rate_prog;
+    const Net n = net_view(smem, p.net);
+    const uint32_t C = p.net.n_comps, V = p.net.n_vars, P = p.net.n_rate_prog;
     const uint32_t bits = ceil_log2(C);
-    const bool rate_table = (n.flags & CSMC_NET_RATE_TABLE) && P > 0;
+    const bool rate_table = (p.net.flags & CSMC_NET_RATE_TABLE) && P > 0;
 
     // per-thread interleaved state
-    uint32_t T, t;
-    uint8_t *st;
-    if (p.state_global) {  // state arrays in global memory, one slab per CTA
-        T = blockDim.x;
-        t = threadIdx.x;
-        st = p.state_global + static_cast<size_t>(blockIdx.x) * p.state_stride;
-    } else {
-        T = blockDim.x;
-        t = threadIdx.x;
-        st = smem + p.blob_bytes;
-    }
+    const uint32_t T = blockDim.x, t = threadIdx.x;
+    uint8_t *st = GSTATE ? p.state_global + static_cast<size_t>(blockIdx.x) * p.state_stride : smem + p.blob_bytes;
     float *fb = reinterpret_cast<float *>(st);
     const VarView vars{fb + t, T};
     const VarView rates{fb + V * T + t, T};
     const VarView shadow{fb + (V + P) * T + t, T};
-    uint16_t *locs = reinterpret_cast<uint16_t *>(st + 4u * (2u * V + P) * T) + t;
-    uint32_t *slotv = reinterpret_cast<uint32_t *>(st + 4u * (2u * V + P) * T + ((2u * C * T + 3u) & ~3u)) + t;
+    const uint32_t loc_bytes = LOC8 ? ((C * T + 3u) & ~3u) : ((2u * C * T + 3u) & ~3u);
+    LocT *locs = reinterpret_cast<LocT *>(st + 4u * (2u * V + P) * T) + t;
+    uint32_t *slotv = reinterpret_cast<uint32_t *>(st + 4u * (2u * V + P) * T + loc_bytes) + t;
+
+    // global location index of component c in local location l / of its stored location
+    auto global_of = [&](uint32_t c, uint32_t stored) -> uint32_t {
+        return LOC8 ? n.comp[c].loc_begin + stored : stored;
+    };
+    auto store_of = [&](uint32_t c, uint32_t local) -> LocT {
+        return static_cast<LocT>(LOC8 ? local : n.comp[c].loc_begin + local);
+    };
 
     const uint32_t lane = threadIdx.x & 31u;
     const float T_end = p.horizon;
@@ -80,7 +97,8 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
         if (want) {
             const int leader = __ffs(want) - 1;
             unsigned long long base = 0;
-            if (static_cast<int>(lane) == leader) base = atomicAdd(p.scratch, static_cast<unsigned long long>(__popc(want)));
+            if (static_cast<int>(lane) == leader)
+                base = atomicAdd(p.scratch, static_cast<unsigned long long>(__popc(want)));
             base = __shfl_sync(act, base, leader);
             if (need) {
                 ridx = base + __popc(want & ((1u << lane) - 1u));
@@ -89,7 +107,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                 run = p.first_run + ridx;
                 // run initialisation (simulation.cu:766-831)
                 for (uint32_t c = 0; c < C; ++c) {
-                    locs[c * T] = static_cast<uint16_t>(n.comp[c].loc_begin + n.comp[c].init_local);
+                    locs[c * T] = store_of(c, n.comp[c].init_local);
                     if (SLOTS) slotv[c * T] = 0u;
                 }
                 for (uint32_t v = 0; v < V; ++v) vars[v] = n.var[v].init;
@@ -119,7 +137,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                 if (p.digests) p.digests[ridx] = sc.digest;
                 if (p.final_state) {
                     uint32_t *w = p.final_state + ridx * (C + V);
-                    for (uint32_t c = 0; c < C; ++c) w[c] = locs[c * T] - n.comp[c].loc_begin;
+                    for (uint32_t c = 0; c < C; ++c) w[c] = global_of(c, locs[c * T]) - n.comp[c].loc_begin;
                     for (uint32_t v = 0; v < V; ++v) w[C + v] = f_bits(vars[v]);
                 }
             }
@@ -139,7 +157,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                 for (uint32_t v = 0; v < V; ++v) shadow[v] = vars[v];
                 for (uint32_t c = 0; c < C; ++c) {
                     if (static_cast<int>(c) == sender) continue;
-                    const uint32_t li = locs[c * T];
+                    const uint32_t li = global_of(c, locs[c * T]);
                     if (!n.loc[li].n_recv) continue;
                     const uint32_t m = recv_edges(n, shadow, li, chan);
                     if (!m) continue;
@@ -152,7 +170,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                     const uint32_t base = n.comp[c].loc_begin;
                     const uint32_t nl =
                         take_edge<VERIFY>(n, vars, sc, p.seed, p.var_id, run, step, c, li - base, m, sm, 1);
-                    locs[c * T] = static_cast<uint16_t>(base + nl);
+                    locs[c * T] = store_of(c, nl);
                 }
             }
             sc.chan = 0;
@@ -176,7 +194,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                     // exponential delay with the literal 1/rate or the
                     // step's evaluated rate; zero-delay types and bounded
                     // locations take the general path
-                    const uint32_t li = locs[cc * T];
+                    const uint32_t li = global_of(cc, locs[cc * T]);
                     const uint64_t dsc = n.loc_desc[li];
                     const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
                     const uint32_t x = word_of(blk, k);
@@ -202,11 +220,11 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             mix(sc.digest, f_bits(dmin));
         }
         if (static_cast<double>(dmin) < kDblMax) {
-            for (uint32_t j = 0; j < n.n_clocks; ++j) {  // simulation.cu:632-651
+            for (uint32_t j = 0; j < p.net.n_clocks; ++j) {  // simulation.cu:632-651
                 const uint32_t v = n.clock[j];
                 vars[v] = d2f(d_add(static_cast<double>(vars[v]), static_cast<double>(dmin)));
             }
-            const uint32_t li = locs[win * T];  // simulation.cu:656-667
+            const uint32_t li = global_of(win, locs[win * T]);  // simulation.cu:656-667
             const uint32_t en = enabled_edges(n, vars, li);
             uint32_t sm = 0;
             if (SLOTS) {
@@ -215,8 +233,9 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             }
             if (en) {
                 const uint32_t base = n.comp[win].loc_begin;
-                const uint32_t nl = take_edge<VERIFY>(n, vars, sc, p.seed, p.var_id, run, step, win, li - base, en, sm, 0);
-                locs[win * T] = static_cast<uint16_t>(base + nl);
+                const uint32_t nl =
+                    take_edge<VERIFY>(n, vars, sc, p.seed, p.var_id, run, step, win, li - base, en, sm, 0);
+                locs[win * T] = store_of(win, nl);
             } else if (VERIFY) {
                 mix(sc.digest, 0xffffffffu);
             }
@@ -232,18 +251,18 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
 
 }  // namespace detail
 
-template <bool VERIFY, bool SLOTS>
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
 int serial_launch_one(const SimParams &p, int grid, int block, size_t smem, void *stream) {
-    auto fn = detail::serial_kernel<VERIFY, SLOTS>;
+    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     fn<<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return static_cast<int>(cudaGetLastError());
 }
 
-template <bool VERIFY, bool SLOTS>
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
 int serial_occupancy_one(int block, size_t smem, int *ctas) {
-    auto fn = detail::serial_kernel<VERIFY, SLOTS>;
+    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     return static_cast<int>(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, smem));

@@ -138,16 +138,17 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         // plan: one thread per run, 128 threads per CTA; run state in shared
         // memory when it fits, otherwise in slabs of the scratch array
         const bool slots = h.max_edges_per_loc >= 2;
+        const bool loc8 = h.max_locs_per_comp <= 256;
         const uint32_t blob_bytes = h.total_bytes;
         if (blob_bytes > static_cast<uint32_t>(max_smem))
             return fail(CSMC_ERR_LIMIT, "network does not fit in shared memory");
         const int block = 128;
-        const size_t per_thread = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, slots);
+        const size_t per_thread = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, slots, loc8);
         const size_t slab = (per_thread * block + 15) & ~static_cast<size_t>(15);
         const bool in_smem = blob_bytes + slab <= static_cast<size_t>(max_smem);
         const size_t smem = in_smem ? blob_bytes + slab : blob_bytes;
         int ctas = 0;
-        rc = csmc::serial_max_active_ctas(false, slots, block, smem, &ctas);
+        rc = csmc::serial_max_active_ctas(false, slots, loc8, !in_smem, block, smem, &ctas);
         if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
         if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network");
         uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(ctas);
@@ -167,6 +168,7 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         e = cudaMemsetAsync(base, 0, kPartialOffset, st);  // counters start at zero
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(scratch)");
         csmc::SimParams p{};
+        p.net = csmc::layout_of(h);
         p.blob = static_cast<const uint8_t *>(blob_device);
         p.blob_bytes = blob_bytes;
         p.state_stride = static_cast<uint32_t>(slab);
@@ -184,7 +186,7 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         p.steps = steps;
         p.scratch = reinterpret_cast<unsigned long long *>(base);
         p.state_global = in_smem ? nullptr : base + kSlabOffset;
-        rc = csmc::serial_launch(false, slots, p, static_cast<int>(grid), block, smem, st);
+        rc = csmc::serial_launch(false, slots, loc8, !in_smem, p, static_cast<int>(grid), block, smem, st);
         if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
         double *partials = reinterpret_cast<double *>(base + kPartialOffset);
         const bool need_values = q->kind == CSMC_QUERY_VARIABLE;
