@@ -2,6 +2,11 @@
 epidemic network, Pr[<=100](<> R >= 50), 1,000,000 runs per step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload epidemic_100|random_0|mutex_8|mutex_32|mutex_64|mutex_256]
+
+The default workload is the epidemic; the others (the small random network
+and the Fischer-style mutex at n = 8, 32, 64, 256) use the same measurement
+with their own run counts (1e4 and 1e7 runs per step).
 
 A step is one pass of the hot path over one batch: 1e6 independent runs of
 the epidemic network (seeded synthetic input: the network comes from
@@ -15,8 +20,9 @@ every rank simulates its own run range (weak scaling, no data-path
 collective); times are the max over ranks.
 
 --impl reference times the reference cuSMC binary, built from the reference
-sources for sm_100a by oracle/ref/Makefile (oracle/_ref/cusmc_ref_v8: limits
-raised to 8 variables / 8 enabled edges), on the same model file and query,
+sources for sm_100a by oracle/ref/Makefile (oracle/_ref/cusmc_ref_v{8,16,64,512}:
+limits raised to that many variables and 8 enabled edges; the smallest build
+that holds the network's variables is used), on the same model file and query,
 from its own "Time taken" report (kernel + synchronise, smc.cu:234-255), on
 rank 0 only.
 """
@@ -37,7 +43,29 @@ sys.path.insert(0, ROOT)
 
 RUNS_PER_STEP = 1_000_000
 SEED = 20241203
-METRIC = "runs/s at 1 B200 (100-agent SEIR epidemic, Pr[<=100](<> R>=50))"
+
+# name -> (generator, description); runs per step default to the workload's
+# own run count (the epidemic: 1e6)
+WORKLOADS = {
+    "epidemic_100": (lambda: _netgen().epidemic(n_agents=100, runs=RUNS_PER_STEP),
+                     "100-agent SEIR epidemic, Pr[<=100](<> R>=50)"),
+    "random_0": (lambda: _netgen().random_network(0, runs=10_000),
+                 "random network seed 0: 8 components x 4 locations x 6 edges, 1 clock each, 2 ints, "
+                 "Pr[<=100](<> v0>=target)"),
+    "mutex_8": (lambda: _netgen().mutex(8), "Fischer-style mutex n=8, Pr[<=200](<> incs>=2)"),
+    "mutex_32": (lambda: _netgen().mutex(32), "Fischer-style mutex n=32, Pr[<=200](<> incs>=2)"),
+    "mutex_64": (lambda: _netgen().mutex(64), "Fischer-style mutex n=64, Pr[<=200](<> incs>=2)"),
+    "mutex_256": (lambda: _netgen().mutex(256), "Fischer-style mutex n=256, Pr[<=200](<> incs>=2)"),
+}
+
+
+def _netgen():
+    from cusmc_b200 import netgen
+    return netgen
+
+
+def metric_of(name):
+    return f"runs/s at 1 B200 ({WORKLOADS[name][1]})"
 
 
 def _env_rank():
@@ -92,14 +120,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def epidemic_blob():
-    from cusmc_b200 import api, netgen
-    w = netgen.epidemic(n_agents=100, runs=RUNS_PER_STEP)
+def workload_blob(name):
+    from cusmc_b200 import api
+    w = WORKLOADS[name][0]()
     d = tempfile.mkdtemp(prefix="csmc_bench_")
-    path = w.write(os.path.join(d, "epidemic_100.xml"))
+    path = w.write(os.path.join(d, name + ".xml"))
     blob = api.compile_model(path)
     q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, is_estimate=False)
     return w, path, blob, q
+
+
+def profile_traffic_per_run(name):
+    """DRAM bytes (read + write) per run of the simulation kernel, from the ncu
+    capture summarised in profiles/ (a smaller launch of the same kernel and
+    network, scaled by runs): the line `dram_bytes_per_run = X`."""
+    p = os.path.join(ROOT, "profiles", f"serial_kernel_{name}.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            line = line.strip().strip("`")
+            if line.startswith("dram_bytes_per_run ="):
+                return float(line.split("=")[1])
+    return None
 
 
 def load_peaks():
@@ -135,9 +178,9 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
-    w, path, blob, q = epidemic_blob()
+    w, path, blob, q = workload_blob(args.workload)
     net = api.Network(blob)
-    n = args.runs
+    n = args.runs or w.runs
     dev = torch.device("cuda", local)
     flags = torch.empty(n, dtype=torch.uint8, device=dev)
     values = torch.empty(n, dtype=torch.float64, device=dev)
@@ -198,32 +241,49 @@ def run_ours(args):
     e2e_value = runs_total / (e2e_t / 1000.0)
 
     peak, peak_kind = load_peaks()
-    # algorithmic HBM bytes of one simulation launch: the network staged once
-    # per CTA plus one flag byte and one 8-byte value per run
+    info = api.blob_info(blob)
+    n_comps = info["n_comps"]
     plan = net.plan()
     lanes, cpl, rpc = plan
-    ctas = min((n + rpc - 1) // rpc, 148 * 8)
-    alg_bytes = len(blob) * ctas + 9 * n
-    achieved = alg_bytes / (t_kernel / args.steps / 1000.0) / 1e9
-    comp_steps = steps_total / world * 100 / args.steps  # component-steps per launch on this rank
+    launch_ms = t_kernel / args.steps
+    # algorithmic HBM bytes of one simulation launch: one flag byte and one
+    # 8-byte value per run written, the network read once
+    alg_bytes = 9 * n + len(blob)
+    achieved = alg_bytes / (launch_ms / 1000.0) / 1e9
+    traffic_per_run = profile_traffic_per_run(args.workload)
+    # the kernel is bound by instruction issue and shared-memory access, not
+    # HBM: one component-step (one component's part in one race) touches
+    # 32 B of run state and network records in shared memory
+    comp_steps = steps_total * n_comps  # all ranks
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    smem_peak = 128.0 * 148 * sm_mhz * 1e6 / 1e9  # GB/s: 128 B/clk/SM
+    smem_achieved = 32.0 * comp_steps / world / (t_kernel / 1000.0) / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_of(args.workload), "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 expressions", "data": "synthetic (seeded generated network)",
-        "config": {"workload": "epidemic_100 (SEIR, 100 agents, beta=0.3, E->I 0.2, I->R 0.1), T=100, "
-                               f"Pr[<=100](<> R>=50), {n} runs per step per GPU",
+        "config": {"workload": f"{args.workload} ({WORKLOADS[args.workload][1]}), {n} runs per step per GPU",
                    "runs_per_step_per_gpu": n, "lanes_per_run": lanes, "comps_per_lane": cpl,
                    "runs_per_cta": rpc, "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"runs sharded over {world} GPU(s)"},
         "estimate": hits / runs_total,
         "race_steps_per_run": steps_total / runs_total,
-        "component_steps_per_s": steps_total * 100 / (t_total / 1000.0),
+        "component_steps_per_s": comp_steps / (t_total / 1000.0),
         "e2e": {"value": e2e_value, "unit": "runs/s", "h2d_bytes_per_step": len(blob),
                 "d2h_bytes_per_step": 9 * n},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                     "note": "issue-bound kernel: HBM bytes per launch are the staged network and 9 B/run "
-                             "of results; see issue figures from ncu in profiles/"},
+                     "frac": achieved / peak,
+                     "traffic": None if traffic_per_run is None else traffic_per_run * n,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
+                     "note": "HBM is not what bounds this kernel (9 B per run of results); the binding "
+                             "resources are instruction issue and shared memory, below"},
+        "issue_roofline": {"bound": "shared memory / issue", "unit": "GB/s",
+                           "bytes_per_component_step": 32, "achieved": smem_achieved, "peak": smem_peak,
+                           "frac": smem_achieved / smem_peak,
+                           "peak_source": f"128 B/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (median SM clock sampled "
+                                          "during the timed steps)"},
         "clocks": clocks,
         "gpu_launches": 2 * args.steps,
         "wall_s": wall,
@@ -242,12 +302,16 @@ def run_reference(args):
     rank, world, _ = _env_rank()
     if rank != 0:
         return
-    binary = os.path.join(ROOT, "oracle", "_ref", "cusmc_ref_v8")
-    if not os.path.exists(binary):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cusmc_ref_v8 was not built "
+    from cusmc_b200 import api
+    w, path, blob, q = workload_blob(args.workload)
+    # the smallest limits build that holds the network's variables
+    n_vars = api.blob_info(blob)["n_vars"]
+    variant = next((v for v in (8, 16, 64, 512) if v >= n_vars), None)
+    binary = os.path.join(ROOT, "oracle", "_ref", f"cusmc_ref_v{variant}")
+    if variant is None or not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/cusmc_ref_v{variant} was not built "
                           "(the reference checkout is needed at build time)"}))
         return
-    w, path, blob, q = epidemic_blob()
     work = tempfile.mkdtemp(prefix="csmc_ref_")
     cwd = os.path.join(work, "run")  # the reference writes ../results5.csv
     os.makedirs(cwd)
@@ -269,7 +333,7 @@ def run_reference(args):
 
     probe_ms, _ = once(20_000, 1)
     rate = 20_000 / (probe_ms / 1000.0)
-    sample = int(min(RUNS_PER_STEP, max(20_000, rate * 10.0)))
+    sample = int(min(args.runs or w.runs, max(20_000, rate * 10.0)))
     for s in range(args.warmup):
         once(sample, 100 + s)
     times, results = [], []
@@ -279,12 +343,12 @@ def run_reference(args):
         results.append(res)
     value = sample * args.steps / (sum(times) / 1000.0)
     line = {
-        "metric": METRIC, "value": value, "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
+        "metric": metric_of(args.workload), "value": value, "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sum(times) / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 state / f64 expressions",
         "data": "synthetic (seeded generated network)", "impl": "reference",
-        "config": {"workload": "epidemic_100 (SEIR, 100 agents), T=100, Pr[<=100](<> R>=50)",
-                   "runs_per_step": sample, "binary": "reference cuSMC built for sm_100a, MAX_VARIABLES=8, "
+        "config": {"workload": f"{args.workload} ({WORKLOADS[args.workload][1]})",
+                   "runs_per_step": sample, "binary": f"reference cuSMC built for sm_100a, MAX_VARIABLES={variant}, "
                                                      "MAX_EDGES_PER_NODE=8"},
         "estimate": statistics.mean(results) if results else None,
         "cpu_baseline": {"value": value, "unit": "runs/s", "cores": 1, "kind": "reference",
@@ -302,8 +366,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline")
-    ap.add_argument("--runs", type=int, default=RUNS_PER_STEP,
-                    help="runs per step per GPU (default 1e6; smaller values are for profiling captures)")
+    ap.add_argument("--runs", type=int, default=0,
+                    help="runs per step per GPU (default: the workload's run count, 1e6 for the epidemic; "
+                         "smaller values are for profiling captures)")
+    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS),
+                    help="network and query (default: the 100-agent epidemic)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
