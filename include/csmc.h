@@ -56,7 +56,7 @@ typedef struct {
     int32_t is_estimate; /* 1: mean of the tracked values; 0: fraction beyond threshold */
     double threshold;    /* probability queries: value > threshold (max) or < threshold (min) */
     double horizon;      /* time bound T */
-    uint64_t max_steps;  /* per-run step cap (0: 2^32-1); capped runs are counted */
+    uint64_t max_steps;  /* per-run race-step cap (0: 10^7); capped runs are counted */
 } csmc_query;
 
 typedef struct {
