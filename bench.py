@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -62,6 +63,11 @@ WORKLOADS = {
 def _netgen():
     from cusmc_b200 import netgen
     return netgen
+
+
+# the rare event of the importance-sampling workload: (T, threshold) with
+# goal R > threshold
+IS_RARE = (100, 94)
 
 
 def metric_of(name):
@@ -359,6 +365,135 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _blob_of(w):
+    from cusmc_b200 import api
+    d = tempfile.mkdtemp(prefix="csmc_bench_")
+    return api.compile_model(w.write(os.path.join(d, w.name + ".xml")))
+
+
+def run_batch(args):
+    """64 seeded random networks (2..512 components, 2..8 locations per
+    automaton, horizons 50..500, budgets 1e3..1e6 runs) in one persistent,
+    graph-captured launch with an autotuned geometry, against the same jobs as
+    64 sequential per-network launches with each network's default plan.
+    value = runs/s of the batched launch; `sequential` = runs/s of the 64
+    launches."""
+    import torch
+    from cusmc_b200 import api, netgen
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    ws = netgen.batch_networks()
+    nets = [api.Network(_blob_of(w)) for w in ws]
+    jobs = []
+    for i, (w, net) in enumerate(zip(ws, nets)):
+        q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=1_000_000)
+        jobs.append((net, q, SEED + i, w.runs, rank * 10 ** 9))
+    total = sum(j[3] for j in jobs)
+    batch = api.Batch(jobs)
+    t_tune = time.perf_counter()
+    geometry = batch.autotune(probe_fraction=0.02)
+    t_tune = time.perf_counter() - t_tune
+    for _ in range(args.warmup):
+        batch.run(use_graph=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    batch_ms = []
+    for _ in range(args.steps):
+        res = batch.run(use_graph=True)
+        batch_ms.append(res[0].kernel_ms)
+    clocks = sampler.stop()
+    # the same jobs as sequential launches
+    seq_ms = []
+    seq_res = None
+    for _ in range(max(1, min(args.steps, 2))):
+        t = 0.0
+        seq_res = []
+        for net, q, seed, runs, first in jobs:
+            r = net.run(q, seed, runs, first)
+            t += r.kernel_ms
+            seq_res.append(r)
+        seq_ms.append(t)
+    same = all(a.hits == b.hits and a.steps == b.steps for a, b in zip(res, seq_res))
+    value = total * args.steps / (sum(batch_ms) / 1000.0)
+    seq_value = total * len(seq_ms) / (sum(seq_ms) / 1000.0)
+    line = {"metric": "runs/s at 1 B200 (64 random networks in one launch)", "value": value, "unit": "runs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(batch_ms) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 state / f64 expressions",
+            "data": "synthetic (64 seeded generated networks)",
+            "config": {"workload": "batch_64 (random networks, seeds 1000..1063)", "runs_per_step": total,
+                       "threads_per_cta": geometry[0], "ctas_per_sm": geometry[1], "graph": True},
+            "sequential": {"value": seq_value, "unit": "runs/s", "ms_per_step": sum(seq_ms) / len(seq_ms)},
+            "speedup_vs_sequential": value / seq_value, "results_identical_to_sequential": same,
+            "autotune_s": t_tune, "clocks": clocks, "gpu_launches": 2 * args.steps}
+    batch.close()
+    for n in nets:
+        n.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_rare_is(args):
+    """The epidemic with a rare goal (R reaches the threshold within T):
+    time to a 10%-relative-error 95% CI, learned importance sampling (CE
+    training on the GPU included) against plain SMC at its measured rate."""
+    import torch
+    from cusmc_b200 import api, netgen, proposal as P
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    w = netgen.epidemic()
+    net = api.Network(_blob_of(w))
+    T, thr = IS_RARE
+    q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
+    t0 = time.perf_counter()
+    prop, log = P.train(net, q, seed=1, rounds=10, runs_per_round=100_000, adam_steps=30, lr=5e-3)
+    train_s = time.perf_counter() - t0
+    # importance sampling until the 95% CI half-width is 10% of the estimate
+    chunk = 1_000_000
+    s1 = s2 = 0.0
+    n = 0
+    t1 = time.perf_counter()
+    while True:
+        r = P.is_run(net, q, prop.pack(), 9, chunk, 2_000_000_000 + n)
+        s1 += r.sum
+        s2 += r.sum_sq
+        n += chunk
+        p = s1 / n
+        half = 1.96 * math.sqrt(max(s2 / n - p * p, 0.0) / n)
+        if (p > 0 and half <= 0.1 * p) or n >= 10_000_000:
+            break
+    is_s = time.perf_counter() - t1
+    # plain SMC: measured rate, and an estimate on a bounded sample
+    plain_n = args.runs or 100_000_000
+    hits = 0
+    t2 = time.perf_counter()
+    done = 0
+    while done < plain_n:
+        m = min(10_000_000, plain_n - done)
+        hits += net.run(q, 13, m, 4_000_000_000 + done).hits
+        done += m
+    plain_s = time.perf_counter() - t2
+    plain_rate = plain_n / plain_s
+    p_plain = hits / plain_n
+    half_plain = 1.96 * math.sqrt(max(p_plain * (1 - p_plain), 0.0) / plain_n)
+    need_plain = 1.96 ** 2 * (1 - p) / (0.01 * p) if p > 0 else float("inf")
+    plain_to_10 = need_plain / plain_rate
+    line = {"metric": "seconds to a 10%-relative-error 95% CI (learned IS vs plain SMC), epidemic rare event",
+            "value": train_s + is_s, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 network / f32 accumulation / f64 log-weights", "data": "synthetic",
+            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1})", "ce_rounds": 10,
+                       "runs_per_round": 100_000},
+            "is": {"estimate": p, "ci_half": half, "runs": n, "train_s": train_s, "sample_s": is_s},
+            "plain": {"estimate": p_plain, "ci_half": half_plain, "runs": plain_n, "runs_per_s": plain_rate,
+                      "runs_for_10pct": need_plain, "seconds_for_10pct": plain_to_10},
+            "speedup": plain_to_10 / (train_s + is_s),
+            "agree": abs(p - p_plain) <= half + half_plain,
+            "ce_log": log.rounds}
+    net.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,9 +504,17 @@ def main():
     ap.add_argument("--runs", type=int, default=0,
                     help="runs per step per GPU (default: the workload's run count, 1e6 for the epidemic; "
                          "smaller values are for profiling captures)")
-    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS),
+    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is"],
                     help="network and query (default: the 100-agent epidemic)")
     args = ap.parse_args()
+    if args.workload == "batch_64" and args.impl == "ours":
+        return run_batch(args)
+    if args.workload == "rare_is" and args.impl == "ours":
+        return run_rare_is(args)
+    if args.workload in ("batch_64", "rare_is"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference simulates one model per process and has "
+                          "no importance sampling; this workload has no reference arm"}))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

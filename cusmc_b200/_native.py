@@ -100,6 +100,36 @@ _SIGNATURES = {
     "csmc_run_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(Query),
                                         ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),
+    "csmc_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_uint64, ctypes.c_uint64,
+                                     ctypes.POINTER(Result)]),
+    "csmc_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Query),
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "csmc_batch_set_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    "csmc_batch_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_int32)]),
+    "csmc_batch_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "csmc_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Result)]),
+    "csmc_batch_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Result)]),
+    "csmc_batch_outputs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
+    "csmc_batch_outputs_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "csmc_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]),
+    "csmc_batch_free": (None, [ctypes.c_void_p]),
+    "csmc_is_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_char_p, ctypes.c_uint64,
+                                   ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),
+    "csmc_is_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_char_p, ctypes.c_uint64,
+                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+    "csmc_mlp_forward": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    "csmc_mlp_grad": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
 }
 
 

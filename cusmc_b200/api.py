@@ -132,8 +132,16 @@ class Network:
     def set_plan(self, family: int, lanes_per_run: int = 32, comps_per_lane: int = 1,
                  threads_per_cta: int = 128) -> None:
         """Selects the kernel family and launch shape (0: lane groups, 1: one
-        thread per run)."""
+        thread per run, 2: one thread per run with the network in global
+        memory)."""
         check(lib().csmc_set_plan(self._h, family, lanes_per_run, comps_per_lane, threads_per_cta))
+
+    def autotune(self, query: Query, seed: int, probe_runs: int) -> Result:
+        """Times every feasible launch plan on runs 0..probe_runs-1 and keeps
+        the fastest (csmc_autotune); returns the winning probe's result."""
+        r = Result()
+        check(lib().csmc_autotune(self._h, ctypes.byref(query), seed & (2**64 - 1), probe_runs, ctypes.byref(r)))
+        return r
 
     def run(self, query: Query, seed: int, n_runs: int, first_run: int = 0, flags=None, values=None, steps=None,
             stream: int | None = None) -> Result:
@@ -168,6 +176,74 @@ class Network:
         return r, out
 
 
+class Batch:
+    """Many (network, query) jobs simulated by one persistent launch
+    (csmc_batch_*).  jobs: list of (Network, Query, seed, n_runs) or
+    (Network, Query, seed, n_runs, first_run)."""
+
+    def __init__(self, jobs, verify: bool = False):
+        n = len(jobs)
+        self.jobs = list(jobs)
+        nets = (ctypes.c_void_p * n)(*[j[0]._h for j in jobs])
+        qs = (Query * n)(*[j[1] for j in jobs])
+        seeds = (ctypes.c_uint64 * n)(*[j[2] & (2**64 - 1) for j in jobs])
+        runs = (ctypes.c_uint64 * n)(*[j[3] for j in jobs])
+        firsts = (ctypes.c_uint64 * n)(*[(j[4] if len(j) > 4 else 0) for j in jobs])
+        h = ctypes.c_void_p()
+        check(lib().csmc_batch_create(nets, qs, seeds, firsts, runs, n, 1 if verify else 0, ctypes.byref(h)))
+        self._h = h
+        self.verify = verify
+
+    def close(self) -> None:
+        if self._h:
+            lib().csmc_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_plan(self, threads_per_cta: int, ctas_per_sm: int = 0) -> None:
+        check(lib().csmc_batch_set_plan(self._h, threads_per_cta, ctas_per_sm))
+
+    def plan(self) -> tuple[int, int]:
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().csmc_batch_plan(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, probe_fraction: float = 0.05) -> tuple[int, int]:
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().csmc_batch_autotune(self._h, probe_fraction, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def run(self, use_graph: bool = True, stream: int | None = None) -> list[Result]:
+        """Runs the whole batch; one Result per job, in job order."""
+        outs = (Result * len(self.jobs))()
+        check(lib().csmc_batch_run(self._h, 1 if use_graph else 0, stream, outs))
+        return list(outs)
+
+    def outputs(self, job: int) -> dict:
+        """Per-run outputs of one job as numpy arrays."""
+        net = self.jobs[job][0]
+        n = self.jobs[job][3]
+        C, V = net.info["n_comps"], net.info["n_vars"]
+        flags = np.zeros(n, dtype=np.uint8)
+        values = np.zeros(n, dtype=np.float64)
+        steps = np.zeros(n, dtype=np.uint32)
+        digests = np.zeros(n, dtype=np.uint64) if self.verify else None
+        final = np.zeros(n * (C + V), dtype=np.uint32) if self.verify else None
+        check(lib().csmc_batch_outputs_host(self._h, job, flags.ctypes.data, values.ctypes.data, steps.ctypes.data,
+                                            None if digests is None else digests.ctypes.data,
+                                            None if final is None else final.ctypes.data))
+        out = {"flags": flags, "values": values, "steps": steps}
+        if self.verify:
+            out["digests"] = digests
+            out["final_state"] = final.reshape(n, C + V)
+        return out
+
+
 def run_host(blob: bytes, query: Query, seed: int, n_runs: int, first_run: int = 0, want_steps: bool = False):
     """Host buffers in and out (upload, kernel, copies back). Returns
     (Result, flags, values, steps-or-None) with numpy arrays."""
@@ -195,7 +271,7 @@ def version() -> str:
 
 
 __all__ = [
-    "Configuration", "StatisticsConfiguration", "Network", "Query", "Result", "compile_model", "dump_model",
+    "Batch", "Configuration", "StatisticsConfiguration", "Network", "Query", "Result", "compile_model", "dump_model",
     "blob_info", "make_query", "location_query", "variable_query", "run_host", "smc", "version",
     "QUERY_LOCATION", "QUERY_VARIABLE", "_native",
 ]

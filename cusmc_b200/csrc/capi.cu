@@ -5,6 +5,8 @@
 #include "include/csmc_net.h"
 #include "include/csmc_numeric.h"
 #include "kernels/sim.cuh"
+#include "kernels/reduce.cuh"
+#include "capi_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -21,31 +23,6 @@
 #include <sstream>
 #include <string>
 #include <vector>
-
-struct csmc_net {
-    int device = 0;
-    uint8_t *d_blob = nullptr;
-    uint32_t bytes = 0;       // staged bytes (multiple of 16)
-    csmc_net_header h{};
-    unsigned long long *d_scratch = nullptr;
-    // internal per-run buffers used when the caller passes none
-    uint8_t *d_flags = nullptr;
-    double *d_values = nullptr;
-    uint64_t cap_runs = 0;
-    double *d_partials = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // launch plan: family 0 = lane groups (lanes, comps_per_lane), 1 = one
-    // thread per run
-    int family = 1;
-    int lanes = 0, comps_per_lane = 0, block = 256, grid = 0;
-    size_t smem = 0;
-    uint32_t state_stride = 0;
-    bool slots = false;
-    bool loc8 = false;  // every automaton has at most 256 locations
-    bool state_in_global = false;
-    uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
-    size_t state_bytes = 0;
-};
 
 namespace {
 
@@ -120,6 +97,25 @@ bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std:
         why = "thread-per-run plans use 32..128 threads per CTA";
         return false;
     }
+    if (family == 2) {  // network and run state in global memory
+        if (h.max_locs_per_comp > 0xffffu || h.n_locs > 0xffffu) {
+            why = "more than 65535 locations";
+            return false;
+        }
+        const size_t per = csmc::batch_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog);
+        n->family = 2;
+        n->lanes = 1;
+        n->comps_per_lane = static_cast<int>(h.n_comps);
+        n->block = block;
+        n->state_stride = static_cast<uint32_t>((per * block + 15) & ~static_cast<size_t>(15));
+        n->state_in_global = true;
+        n->smem = csmc::batch_smem_bytes(1);
+        return true;
+    }
+    if (family != 1) {
+        why = "unknown plan family";
+        return false;
+    }
     if (n->bytes > max_smem) {
         why = "network does not fit in shared memory";
         return false;
@@ -161,33 +157,9 @@ int ensure_buffers(csmc_net *n, uint64_t runs) {
     return CSMC_OK;
 }
 
-// Deterministic sum and sum of squares of values[0..n): fixed chunking,
-// fixed per-thread order and a fixed shared-memory tree.
-constexpr int kReduceBlocks = 256;
+using csmc::kReduceBlocks;
 __global__ void reduce_values(const double *values, uint64_t n, double *partials) {
-    __shared__ double s1[256], s2[256];
-    const uint64_t chunk = (n + kReduceBlocks - 1) / kReduceBlocks;
-    const uint64_t b0 = blockIdx.x * chunk, b1 = (b0 + chunk < n) ? b0 + chunk : n;
-    double a = 0.0, q = 0.0;
-    for (uint64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        const double v = values[i];
-        a = csmc::d_add(a, v);
-        q = csmc::d_add(q, csmc::d_mul(v, v));
-    }
-    s1[threadIdx.x] = a;
-    s2[threadIdx.x] = q;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            s1[threadIdx.x] = csmc::d_add(s1[threadIdx.x], s1[threadIdx.x + s]);
-            s2[threadIdx.x] = csmc::d_add(s2[threadIdx.x], s2[threadIdx.x + s]);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = s1[0];
-        partials[2 * blockIdx.x + 1] = s2[0];
-    }
+    csmc::reduce_block(values, n, blockIdx.x, partials + 2 * blockIdx.x);
 }
 
 int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t first_run, uint64_t n_runs,
@@ -238,7 +210,9 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     p.scratch = n->d_scratch;
     int ctas = 0;
     int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
-                            : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->block, n->smem, &ctas);
+             : n->family == 2 ? csmc::batch_max_active_ctas(verify, n->block, n->smem, &ctas)
+                              : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->block,
+                                                             n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network (shared memory)");
     int sms = 0;
@@ -249,7 +223,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     if (grid > needed) grid = needed;
     n->grid = static_cast<int>(grid);
     p.state_global = nullptr;
-    if (n->family == 1 && n->state_in_global) {
+    if (n->family >= 1 && n->state_in_global) {
         const size_t need = grid * static_cast<size_t>(n->state_stride);
         if (need > n->state_bytes) {
             cudaFree(n->d_state);
@@ -261,10 +235,45 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
         p.state_global = n->d_state;
     }
     p.state_stride = n->state_stride;
+    csmc::BatchParams bp{};
+    if (n->family == 2) {  // the batch kernel with a one-job table
+        if (!n->d_job) CK(cudaMalloc(&n->d_job, sizeof(csmc::BatchJob)), "cudaMalloc(job table)");
+        csmc::BatchJob job{};
+        job.net = p.net;
+        job.blob = n->d_blob;
+        job.run_begin = 0;
+        job.n_runs = n_runs;
+        job.first_run = first_run;
+        job.seed = seed;
+        job.max_steps = p.max_steps;
+        job.threshold = p.threshold;
+        job.horizon = p.horizon;
+        job.loc_mode = p.loc_mode;
+        job.var_id = p.var_id;
+        job.is_max = p.is_max;
+        job.flags = flags;
+        job.values = values;
+        job.steps = steps;
+        job.digests = digests;
+        job.final_state = final_state;
+        job.counters = n->d_scratch + 1;  // hits, steps, capped
+        CK(cudaMemcpyAsync(n->d_job, &job, sizeof job, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(job table)");
+        bp.jobs = n->d_job;
+        bp.n_jobs = 1;
+        bp.state_stride = n->state_stride;
+        bp.total_runs = n_runs;
+        bp.queue = n->d_scratch;
+        bp.state = n->d_state;
+        bp.max_vars = n->h.n_vars;
+        bp.max_rate_prog = n->h.n_rate_prog;
+        bp.max_comps = n->h.n_comps;
+    }
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
-    rc = n->family == 0
-             ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block, n->smem, st)
-             : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, p, static_cast<int>(grid), n->block, n->smem, st);
+    rc = n->family == 0   ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block,
+                                             n->smem, st)
+         : n->family == 2 ? csmc::batch_launch(verify, bp, static_cast<int>(grid), n->block, st)
+                          : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, p,
+                                                static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
     if (need_values) reduce_values<<<kReduceBlocks, 256, 0, st>>>(values, n_runs, n->d_partials);
@@ -425,6 +434,7 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     if (serial_fits) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
     if (!ok) ok = configure_plan(n.get(), 0, G, K, 256, why);
     if (!ok) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
+    if (!ok) ok = configure_plan(n.get(), 2, 1, static_cast<int>(h->n_comps), 128, why);
     if (!ok) return fail(CSMC_ERR_LIMIT, "no launch plan for this network: " + why);
     CK(cudaMalloc(&n->d_blob, n->bytes), "cudaMalloc(network)");
     CK(cudaMemset(n->d_blob, 0, n->bytes), "cudaMemset");
@@ -445,6 +455,10 @@ void csmc_net_free(csmc_net *n) {
     cudaFree(n->d_values);
     cudaFree(n->d_partials);
     cudaFree(n->d_state);
+    cudaFree(n->d_job);
+    cudaFree(n->d_mlp);
+    cudaFree(n->d_wvals);
+    cudaFree(n->d_is_flags);
     if (n->ev0) cudaEventDestroy(n->ev0);
     if (n->ev1) cudaEventDestroy(n->ev1);
     delete n;

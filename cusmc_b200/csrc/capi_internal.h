@@ -1,0 +1,46 @@
+// Internal to libcsmc: the device network handle behind csmc_net (shared by
+// capi.cu and capi_batch.cu).
+#pragma once
+#include "../../include/csmc.h"
+#include "include/csmc_net.h"
+#include "kernels/sim.cuh"
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+struct csmc_net {
+    int device = 0;
+    uint8_t *d_blob = nullptr;
+    uint32_t bytes = 0;       // staged bytes (multiple of 16)
+    csmc_net_header h{};
+    unsigned long long *d_scratch = nullptr;
+    // internal per-run buffers used when the caller passes none
+    uint8_t *d_flags = nullptr;
+    double *d_values = nullptr;
+    uint64_t cap_runs = 0;
+    double *d_partials = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // launch plan: family 0 = lane groups (lanes, comps_per_lane), 1 = one
+    // thread per run, 2 = one thread per run with the network read from
+    // global memory (the batch kernel with one job)
+    int family = 1;
+    int lanes = 0, comps_per_lane = 0, block = 256, grid = 0;
+    size_t smem = 0;
+    uint32_t state_stride = 0;
+    bool slots = false;
+    bool loc8 = false;  // every automaton has at most 256 locations
+    bool state_in_global = false;
+    uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
+    size_t state_bytes = 0;
+    csmc::BatchJob *d_job = nullptr;  // family 2: the one-job table
+    // importance sampling
+    csmc::MlpParams *d_mlp = nullptr;  // the proposal network
+    double *d_wvals = nullptr;         // per run: flag * likelihood ratio
+    uint8_t *d_is_flags = nullptr;
+    uint64_t is_cap = 0;
+};
+
+namespace csmc {
+void set_last_error(const std::string &m);  // capi.cu
+}

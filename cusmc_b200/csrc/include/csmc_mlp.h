@@ -1,0 +1,178 @@
+/*
+ * The proposal network of importance sampling, as plain arithmetic shared by
+ * the CPU oracle and the CUDA kernels (same operations in the same order,
+ * so both give the same bits).
+ *
+ * Proposal.  In a run simulated under the proposal, every component whose
+ * delay is exponential draws it with its rate multiplied by exp(theta),
+ * theta = MLP(features) clipped to [-CSMC_MLP_THETA_MAX, CSMC_MLP_THETA_MAX].
+ * Uniform (invariant-bounded) and zero delays, edge choices and updates are
+ * unchanged.  The run carries the log-likelihood ratio of its path (nominal
+ * over proposal) in FP64, so weight * goal indicator is an unbiased estimate
+ * of the goal probability.
+ *
+ * Features of a component (CSMC_MLP_IN = 16 inputs, 10 used):
+ *   [0..3]  one-hot of its local location index modulo 4
+ *   [4]     its clock value / T (0: components carry no clock feature in
+ *           this build; the slot is kept so trained networks stay valid)
+ *   [5..8]  integer variables 0..3 divided by the number of components
+ *           (for the epidemic network: the S, E, I, R fractions)
+ *   [9]     time / T
+ * rounded to BF16.  All components in the same local location share their
+ * features, so a run needs one network evaluation per location class and
+ * step.
+ *
+ * Network: 16 -> 64 (GELU) -> 64 (GELU) -> 1, BF16 weights, FP32
+ * accumulation; the first hidden layer's activations are rounded to BF16
+ * (the tensor-core training kernels consume them in BF16).  GELU is the tanh
+ * form x * sigmoid(2 * sqrt(2/pi) * (x + 0.044715 x^3)) with the exponential
+ * evaluated by the project's own exp2 (range reduction to [-1/2, 1/2] and a
+ * degree-7 Taylor polynomial of e^(f ln 2)).
+ */
+#ifndef CSMC_MLP_H
+#define CSMC_MLP_H
+
+#include "csmc_numeric.h"
+
+#define CSMC_MLP_IN 16
+#define CSMC_MLP_HID 64
+#define CSMC_MLP_FEATURES 10
+#define CSMC_MLP_THETA_MAX 4.0f
+#define CSMC_MLP_CLASSES 4
+
+namespace csmc {
+
+/* Parameter block (all BF16 bit patterns except where noted), as uploaded:
+ *   w1[HID][IN]   layer 1, row = output unit
+ *   b1[HID]       FP32
+ *   w2[HID][HID]  layer 2, row = output unit
+ *   b2[HID]       FP32
+ *   w3[HID]       FP32 output weights (applied on CUDA cores)
+ *   b3            FP32 */
+struct MlpParams {
+    uint16_t w1[CSMC_MLP_HID][CSMC_MLP_IN];
+    float b1[CSMC_MLP_HID];
+    uint16_t w2[CSMC_MLP_HID][CSMC_MLP_HID];
+    float b2[CSMC_MLP_HID];
+    float w3[CSMC_MLP_HID];
+    float b3;
+    float pad[3];
+};
+static_assert(sizeof(MlpParams) == 11024, "parameter block layout (CSMC_MLP_PARAM_BYTES)");
+
+CSMC_HD float bf16_to_f(uint16_t h) { return bits_f(static_cast<uint32_t>(h) << 16); }
+
+/* FP32 -> BF16, round to nearest even (NaN kept quiet). */
+CSMC_HD uint16_t f_to_bf16(float x) {
+    const uint32_t b = f_bits(x);
+    if ((b & 0x7fffffffu) > 0x7f800000u) return static_cast<uint16_t>((b >> 16) | 0x40u);
+    const uint32_t r = b + 0x7fffu + ((b >> 16) & 1u);
+    return static_cast<uint16_t>(r >> 16);
+}
+
+CSMC_HD float bf16_round(float x) { return bf16_to_f(f_to_bf16(x)); }
+
+/* 2^t for t in [-126, 126] (clamped): t = n + f, |f| <= 1/2, 2^f = e^(f ln2)
+ * by its Taylor polynomial to degree 7 (relative error below 1e-8). */
+CSMC_HD float exp2_f(float t) {
+    t = t < -126.0f ? -126.0f : (t > 126.0f ? 126.0f : t);
+    const float n = static_cast<float>(static_cast<int>(t >= 0.0f ? f_add(t, 0.5f) : f_add(t, -0.5f)));
+    const float g = f_mul(f_add(t, -n), 0.693147182f);
+    float p = 1.98412701e-4f;        // 1/5040
+    p = f_fma(p, g, 1.38888892e-3f);  // 1/720
+    p = f_fma(p, g, 8.33333377e-3f);  // 1/120
+    p = f_fma(p, g, 4.16666679e-2f);  // 1/24
+    p = f_fma(p, g, 0.166666672f);    // 1/6
+    p = f_fma(p, g, 0.5f);
+    p = f_fma(p, g, 1.0f);
+    p = f_fma(p, g, 1.0f);
+    const int e = static_cast<int>(n);
+    return f_mul(p, bits_f(static_cast<uint32_t>(e + 127) << 23));
+}
+
+/* sigmoid(s) = 1 / (1 + 2^(-s log2 e)) */
+CSMC_HD float sigmoid_f(float s) { return f_div(1.0f, f_add(1.0f, exp2_f(f_mul(s, -1.44269502f)))); }
+
+/* GELU, tanh form, and its derivative. */
+CSMC_HD float gelu_arg(float x) {
+    const float x3 = f_mul(f_mul(x, x), x);
+    return f_mul(1.59576912f, f_fma(0.044715f, x3, x));
+}
+CSMC_HD float gelu_f(float x) { return f_mul(x, sigmoid_f(gelu_arg(x))); }
+CSMC_HD float gelu_grad_f(float x) {
+    const float s = sigmoid_f(gelu_arg(x));
+    const float ds = f_mul(s, f_add(1.0f, -s));                              // sigmoid'
+    const float dz = f_mul(1.59576912f, f_fma(f_mul(0.134145f, x), x, 1.0f));  // d(arg)/dx
+    return f_fma(f_mul(x, ds), dz, s);
+}
+
+/* Features of location class l (local index modulo 4) given the run's
+ * variables v[0..3] (n_int of them present), components C, time t and
+ * horizon T; BF16-rounded. */
+CSMC_HD void mlp_features(uint32_t l, const float *v, uint32_t n_int, uint32_t C, float t, float T, float *x) {
+    for (int i = 0; i < CSMC_MLP_IN; ++i) x[i] = 0.0f;
+    x[l & 3u] = 1.0f;
+    const float inv_c = f_div(1.0f, static_cast<float>(C));
+    for (uint32_t i = 0; i < 4 && i < n_int; ++i) x[5 + i] = bf16_round(f_mul(v[i], inv_c));
+    x[9] = bf16_round(f_div(t, T));
+}
+
+/* theta for one feature row: first layer and GELU, activations rounded to
+ * BF16, second layer and GELU, output dot product, clip. */
+CSMC_HD float mlp_theta(const MlpParams &P, const float *x) {
+    float h1[CSMC_MLP_HID];
+    for (int j = 0; j < CSMC_MLP_HID; ++j) {
+        float z = P.b1[j];
+        for (int i = 0; i < CSMC_MLP_IN; ++i) z = f_fma(x[i], bf16_to_f(P.w1[j][i]), z);
+        h1[j] = bf16_round(gelu_f(z));
+    }
+    float th = P.b3;
+    for (int k = 0; k < CSMC_MLP_HID; ++k) {
+        float z = P.b2[k];
+        for (int j = 0; j < CSMC_MLP_HID; ++j) z = f_fma(h1[j], bf16_to_f(P.w2[k][j]), z);
+        th = f_fma(gelu_f(z), P.w3[k], th);
+    }
+    return th < -CSMC_MLP_THETA_MAX ? -CSMC_MLP_THETA_MAX : (th > CSMC_MLP_THETA_MAX ? CSMC_MLP_THETA_MAX : th);
+}
+
+/* Multiplier of 1/rate under the proposal: e^(-theta). */
+CSMC_HD float tilt_factor(float theta) { return exp2_f(f_mul(theta, -1.44269502f)); }
+
+/* An exponential delay is tilted when its 1/rate is finite and positive. */
+CSMC_HD bool tiltable(float inv) { return inv > 0.0f && inv < bits_f(0x7f800000u); }
+
+/* 1/inv' - 1/inv: the change of one component's rate (log2 units). */
+CSMC_HD double rate_change(float inv, float invp) {
+    return d_sub(d_div(1.0, static_cast<double>(invp)), d_div(1.0, static_cast<double>(inv)));
+}
+
+/* Log-likelihood ratio (nominal over proposal) of one race step that took
+ * time d: ln2 * d * sum_c (1/inv'_c - 1/inv_c) + [winner tilted] ln(inv'_w / inv_w)
+ * (delays are -log2(u) * inv, i.e. exponential with rate ln2 / inv). */
+CSMC_HD double step_log_ratio(double rate_change_sum, float d, bool win_tilted, float inv_w, float invp_w) {
+    const double ln2 = 0.6931471805599453;
+    double r = d_mul(d_mul(ln2, rate_change_sum), static_cast<double>(d));
+    if (win_tilted)
+        r = d_add(r, d_mul(ln2, log2_d(d_div(static_cast<double>(invp_w), static_cast<double>(inv_w)))));
+    return r;
+}
+
+/* Training row of one location class in one step of a replayed run with CE
+ * weight w: a = w * ln2 * d * sum over the class's tilted components of
+ * 1/inv (nominal), b = w * [the winner is tilted and in the class].  The
+ * derivative of the path's log-likelihood under the proposal with respect
+ * to the class's theta is then b/w - (a/w) e^theta. */
+CSMC_HD float row_a(double inv_sum, float d, float w) {
+    const double ln2 = 0.6931471805599453;
+    return d2f(d_mul(d_mul(d_mul(ln2, inv_sum), static_cast<double>(d)), static_cast<double>(w)));
+}
+
+/* Row record of the training set. */
+struct MlpRow {
+    uint16_t x[CSMC_MLP_IN];  /* BF16 features */
+    float a, b;
+};
+
+}  // namespace csmc
+
+#endif

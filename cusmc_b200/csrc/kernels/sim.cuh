@@ -24,6 +24,7 @@
 
 #include "../include/csmc_net.h"
 #include "../include/csmc_numeric.h"
+#include "../include/csmc_mlp.h"
 
 namespace csmc {
 
@@ -82,6 +83,82 @@ bool sim_supported(int lanes_per_run, int comps_per_lane);
 int serial_launch(bool verify, bool slots, bool loc8, bool gstate, const SimParams &p, int grid, int block,
                   size_t smem, void *stream);
 int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, int block, size_t smem, int *ctas);
+
+// ---- Multi-network batch kernel (sim_batch.cuh) ---------------------------
+// One persistent launch simulates the runs of many (network, query) jobs.
+// The runs of all jobs form one index space (job j owns [run_begin,
+// run_begin + n_runs)); every lane takes its next run from one device
+// counter, so a lane moves on to the next job the moment the current one has
+// no runs left, whatever the other lanes are doing.  Networks are read from
+// global memory (L1/L2-cached), run state lives in per-CTA global slabs laid
+// out for the largest job.  Results depend only on (job, run index), not on
+// which lane ran it.
+struct BatchJob {
+    NetLayout net;
+    const uint8_t *blob;           // the job's packed network (device, 16-byte aligned)
+    uint64_t run_begin;            // first index of the job in the batch's run space
+    uint64_t n_runs;
+    uint64_t first_run;            // stream index of the job's first run
+    uint64_t seed;
+    uint64_t max_steps;
+    double threshold;
+    float horizon;
+    int32_t loc_mode, var_id, is_max;
+    uint8_t *flags;                // per-run outputs of the job (may be null)
+    double *values;
+    uint32_t *steps;
+    uint64_t *digests;             // verification outputs (may be null)
+    uint32_t *final_state;
+    unsigned long long *counters;  // [0] hits [1] steps [2] capped
+    uint64_t pad;
+};
+static_assert(sizeof(BatchJob) % 16 == 0, "BatchJob is copied in 16-byte words");
+
+struct BatchParams {
+    const BatchJob *jobs;          // device job table, sorted by run_begin
+    uint32_t n_jobs;
+    uint32_t state_stride;         // bytes of one CTA's state slab
+    uint64_t total_runs;
+    unsigned long long *queue;     // the shared run counter
+    uint8_t *state;                // grid * state_stride bytes
+    uint32_t max_vars, max_rate_prog, max_comps, pad;
+};
+
+#define CSMC_BATCH_MAX_JOBS 256
+
+int batch_launch(bool verify, const BatchParams &p, int grid, int block, void *stream);
+int batch_max_active_ctas(bool verify, int block, size_t smem, int *ctas);
+inline size_t batch_smem_bytes(uint32_t n_jobs) { return static_cast<size_t>(n_jobs) * sizeof(BatchJob); }
+// Bytes of one thread's state in a batch slab (16-bit locations, slot masks).
+inline size_t batch_state_bytes_per_thread(uint32_t max_comps, uint32_t max_vars, uint32_t max_rate_prog) {
+    return 4u * (2u * max_vars + max_rate_prog) + 2u * max_comps + 4u * max_comps + 4u;
+}
+
+// ---- Importance sampling (sim_is.cuh) --------------------------------------
+// The thread-per-run kernel under the proposal network; trace mode replays
+// listed runs and writes their CE training rows.
+struct IsParams {
+    SimParams s;                  // network, query, run range; s.values: tracked values
+    const MlpParams *mlp;         // proposal network (device)
+    double *logw;                 // per run: log-likelihood ratio (may be null)
+    double *wvals;                // per run: flag * exp(logw) (may be null)
+    const uint64_t *trace_runs;   // trace mode: run offsets from s.first_run, s.n_runs of them
+    const float *trace_w;         // trace mode: CE weight per listed run
+    const uint64_t *row_offset;   // trace mode: first row of each listed run (4 rows per step)
+    MlpRow *rows;                 // trace mode: the rows
+};
+
+int is_launch(bool trace, bool slots, bool loc8, const IsParams &p, int grid, int block, size_t smem, void *stream);
+int is_max_active_ctas(bool trace, bool slots, bool loc8, int block, size_t smem, int *ctas);
+// Shared memory of the importance-sampling kernel besides network and state.
+size_t is_mlp_smem_bytes();
+
+// Tensor-core kernels of the proposal network (mlp_train.cu): mode 0 writes
+// theta per row, mode 1 gradient partials per CTA (mlp_tc_partial_floats()
+// floats each) and the objective per CTA.
+int mlp_tc_launch(int mode, const MlpRow *rows, uint64_t n_rows, const MlpParams *P, float *theta_out,
+                  float *partials, double *objective, int *error, int grid, void *stream);
+int mlp_tc_partial_floats();
 
 // Bytes of thread-per-run state per thread for a network.
 inline size_t serial_state_bytes_per_thread(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots,

@@ -1,0 +1,243 @@
+// One run owned by one thread: the state layout and the step of the
+// thread-per-run kernels (the single-network kernel of sim_serial.cuh and
+// the multi-network batch kernel of sim_batch.cuh share these, force-inlined).
+//
+// Per-run state lives in interleaved arrays (element i of thread t at
+// [i * T + t]; conflict-free in shared memory, coalesced in global memory):
+// variables, the evaluated rate table, a snapshot of the variables for
+// broadcast receivers, component locations and, when some location has
+// several edges, the enabled-edge slot masks.
+//
+// The component order, the race tie-break, the Philox draws and every
+// arithmetic step follow the reference kernel (simulation/simulation.cu:
+// 674-901) and are those of the lane-group kernel and the CPU oracle.
+#pragma once
+#include "sim_common.cuh"
+
+namespace csmc {
+namespace detail {
+
+// Delay of a component whose location is invariant-bounded, or whose rate
+// is evaluated per component (uncommon; out of line).
+static __device__ __noinline__ float slow_delay(const Net &n, VarView vars, VarView rates, uint32_t li, uint32_t x) {
+    return comp_delay(n, vars, rates, li, x);
+}
+
+template <bool LOC8>
+struct LocStore {
+    using T = uint16_t;  // global location index
+};
+template <>
+struct LocStore<true> {
+    using T = uint8_t;  // local location index
+};
+
+// Views of one thread's run state.  LOC8: locations stored as 8-bit local
+// indices (automata of at most 256 locations), else 16-bit global indices.
+template <bool LOC8>
+struct RunView {
+    using LocT = typename LocStore<LOC8>::T;
+    VarView vars, rates, shadow;
+    LocT *locs;       // this thread's element 0; stride T
+    uint32_t *slotv;  // this thread's element 0; stride T
+    uint32_t T;
+
+    // global location index of component c
+    __device__ __forceinline__ uint32_t loc(const Net &n, uint32_t c) const {
+        return LOC8 ? n.comp[c].loc_begin + locs[c * T] : locs[c * T];
+    }
+    __device__ __forceinline__ void set_local(const Net &n, uint32_t c, uint32_t local) const {
+        locs[c * T] = static_cast<LocT>(LOC8 ? local : n.comp[c].loc_begin + local);
+    }
+};
+
+// Bytes of one thread's run state with V variables, P rate programs and C
+// components (the layout carve_run_view uses).
+static __host__ __device__ __forceinline__ uint32_t run_loc_bytes(uint32_t C, uint32_t T, bool loc8) {
+    return loc8 ? ((C * T + 3u) & ~3u) : ((2u * C * T + 3u) & ~3u);
+}
+
+// Carves thread t's views out of a state slab of T threads laid out as
+// vars[V] | rates[P] | shadow[V] (floats) | locs[C] | slots[C] (u32).
+template <bool LOC8>
+static __device__ __forceinline__ RunView<LOC8> carve_run_view(uint8_t *st, uint32_t V, uint32_t P, uint32_t C,
+                                                                 uint32_t T, uint32_t t) {
+    using LocT = typename LocStore<LOC8>::T;
+    float *fb = reinterpret_cast<float *>(st);
+    RunView<LOC8> r;
+    r.vars = VarView{fb + t, T};
+    r.rates = VarView{fb + V * T + t, T};
+    r.shadow = VarView{fb + (V + P) * T + t, T};
+    r.locs = reinterpret_cast<LocT *>(st + 4u * (2u * V + P) * T) + t;
+    r.slotv = reinterpret_cast<uint32_t *>(st + 4u * (2u * V + P) * T + run_loc_bytes(C, T, LOC8)) + t;
+    r.T = T;
+    return r;
+}
+
+// Run initialisation (simulation.cu:766-831): initial locations, slot
+// masks, initial variable values, query extremes.
+template <bool SLOTS, bool LOC8>
+static __device__ __forceinline__ void run_init(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+                                                RunScalars &sc, int var_id) {
+    for (uint32_t c = 0; c < C; ++c) {
+        rv.set_local(n, c, n.comp[c].init_local);
+        if (SLOTS) rv.slotv[c * rv.T] = 0u;
+    }
+    for (uint32_t v = 0; v < V; ++v) rv.vars[v] = n.var[v].init;
+    double q0 = 0.0;
+    if (var_id >= 0 && static_cast<uint32_t>(var_id) < V && n.var[var_id].kind == 0)
+        q0 = static_cast<double>(n.var[var_id].init);
+    sc = RunScalars{q0, q0, 0xcbf29ce484222325ull, 0, -1, 0, 0};
+}
+
+// Per-run outcome at the end of a run (simulation.cu:835-849, 887-893).
+struct RunEnd {
+    bool done;
+    uint32_t flag, capped;
+    double value;
+};
+
+static __device__ __forceinline__ RunEnd run_end(const RunScalars &sc, float time, float horizon, uint32_t step,
+                                                 uint64_t cap, int loc_mode, int is_max, double threshold) {
+    RunEnd r;
+    const bool timeout = !(time < horizon);
+    const bool at_goal = loc_mode && sc.goal;
+    const bool at_cap = step >= cap;
+    r.done = timeout || at_goal || at_cap;
+    r.capped = (!timeout && !at_goal && at_cap) ? 1u : 0u;
+    r.value = is_max ? sc.qmax : sc.qmin;
+    r.flag = (!timeout && at_goal) ? 1u : 0u;
+    if (!loc_mode) r.flag = is_max ? (r.value > threshold) : (r.value < threshold);
+    return r;
+}
+
+// Final state for verification: local locations, then variable bits.
+template <bool LOC8>
+static __device__ __forceinline__ void run_final_state(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+                                                       uint32_t *w) {
+    for (uint32_t c = 0; c < C; ++c) w[c] = rv.loc(n, c) - n.comp[c].loc_begin;
+    for (uint32_t v = 0; v < V; ++v) w[C + v] = f_bits(rv.vars[v]);
+}
+
+// Pending broadcast receivers of the previous step's sender (SyncInSerial,
+// simulation.cu:357-407): enabled sets from the state the sender left (the
+// snapshot), then transitions in component order on the live state.
+template <bool VERIFY, bool SLOTS, bool LOC8>
+static __device__ __forceinline__ void run_receivers(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+                                                     RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
+                                                     uint32_t step) {
+    if (sc.chan <= 0) return;
+    const uint32_t T = rv.T;
+    const int chan = sc.chan, sender = sc.sender;
+    if (has_receivers(n, chan)) {
+        for (uint32_t v = 0; v < V; ++v) rv.shadow[v] = rv.vars[v];
+        for (uint32_t c = 0; c < C; ++c) {
+            if (static_cast<int>(c) == sender) continue;
+            const uint32_t li = rv.loc(n, c);
+            if (!n.loc[li].n_recv) continue;
+            const uint32_t m = recv_edges(n, rv.shadow, li, chan);
+            if (!m) continue;
+            uint32_t sm = 0;
+            if (SLOTS) {
+                sm = write_slots(rv.slotv[c * T], m);
+                rv.slotv[c * T] = sm;
+            }
+            if (VERIFY) mix(sc.digest, c | 0x80000000u);
+            const uint32_t base = n.comp[c].loc_begin;
+            const uint32_t nl = take_edge<VERIFY>(n, rv.vars, sc, seed, var_id, run, step, c, li - base, m, sm, 1);
+            rv.set_local(n, c, nl);
+        }
+    }
+    sc.chan = 0;
+    sc.sender = -1;
+}
+
+// The race's outcome applied (simulation.cu:632-667, 876-882): clocks
+// advance by dmin, the winner takes an enabled edge, time advances.
+template <bool VERIFY, bool SLOTS, bool LOC8>
+static __device__ __forceinline__ void run_commit(const Net &n, uint32_t n_clocks, const RunView<LOC8> &rv,
+                                                  RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
+                                                  uint32_t &step, float &time, uint32_t win, float dmin) {
+    const uint32_t T = rv.T;
+    const VarView vars = rv.vars;
+    if (VERIFY) {
+        mix(sc.digest, step);
+        mix(sc.digest, win);
+        mix(sc.digest, f_bits(dmin));
+    }
+    if (static_cast<double>(dmin) < kDblMax) {
+        for (uint32_t j = 0; j < n_clocks; ++j) {
+            const uint32_t v = n.clock[j];
+            vars[v] = d2f(d_add(static_cast<double>(vars[v]), static_cast<double>(dmin)));
+        }
+        const uint32_t li = rv.loc(n, win);
+        const uint32_t en = enabled_edges(n, vars, li);
+        uint32_t sm = 0;
+        if (SLOTS) {
+            sm = write_slots(rv.slotv[win * T], en);
+            rv.slotv[win * T] = sm;
+        }
+        if (en) {
+            const uint32_t base = n.comp[win].loc_begin;
+            const uint32_t nl = take_edge<VERIFY>(n, vars, sc, seed, var_id, run, step, win, li - base, en, sm, 0);
+            rv.set_local(n, win, nl);
+        } else if (VERIFY) {
+            mix(sc.digest, 0xffffffffu);
+        }
+    }
+    time = d2f(d_add(static_cast<double>(time), static_cast<double>(dmin)));
+    ++step;
+}
+
+// One step of a run: pending broadcast receivers, the per-step rate table,
+// the race, the clock advance and the winner's transition, the time update.
+template <bool VERIFY, bool SLOTS, bool LOC8>
+static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32_t V, uint32_t P, uint32_t n_clocks,
+                                                bool rate_table, const RunView<LOC8> &rv, RunScalars &sc,
+                                                uint64_t seed, int var_id, uint64_t run, uint32_t &step,
+                                                float &time) {
+    const uint32_t bits = ceil_log2(C);
+    const VarView vars = rv.vars, rates = rv.rates;
+    run_receivers<VERIFY, SLOTS, LOC8>(n, C, V, rv, sc, seed, var_id, run, step);
+
+    // ---- distinct rate programs, once per step
+    if (rate_table)
+        for (uint32_t j = 0; j < P; ++j) rates[j] = inv_rate(eval(n, vars, n.rate_prog[j]));
+
+    // ---- delays and the race (simulation.cu:409-628)
+    unsigned long long best = ~0ull;
+    float bestd = 0.0f;
+    for (uint32_t c = 0; c < C; c += 4) {
+        const u32x4 blk = delay_block(seed, run, step, c >> 2);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t cc = c + k;
+            if (cc < C) {
+                // fast path from the location's delay descriptor: the
+                // exponential delay with the literal 1/rate or the step's
+                // evaluated rate; zero-delay types and bounded locations
+                // take the general path
+                const uint32_t li = rv.loc(n, cc);
+                const uint64_t dsc = n.loc_desc[li];
+                const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
+                const uint32_t x = word_of(blk, k);
+                float inv = __uint_as_float(lo);
+                if (fl & CSMC_DESC_PROG) inv = rates[lo];
+                float d = exp_delay(x, inv);
+                if (fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL))
+                    d = (fl & CSMC_DESC_ZERO) ? 0.0f : slow_delay(n, vars, rates, li, x);
+                const unsigned long long key =
+                    (static_cast<unsigned long long>(delay_key(d)) << 32) | bitrev_bits(cc, bits);
+                if (key < best) {
+                    best = key;
+                    bestd = d;
+                }
+            }
+        }
+    }
+    const uint32_t win = bitrev_bits(static_cast<uint32_t>(best & 0xffffffffull), bits);
+    run_commit<VERIFY, SLOTS, LOC8>(n, n_clocks, rv, sc, seed, var_id, run, step, time, win, bestd);
+}
+
+}  // namespace detail
+}  // namespace csmc

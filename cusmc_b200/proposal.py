@@ -1,0 +1,240 @@
+"""Learned importance sampling: the proposal network, its parameter block,
+and the cross-entropy (CE) training loop.
+
+The proposal multiplies every exponential rate by exp(theta), theta =
+MLP(features) (cusmc_b200/csrc/include/csmc_mlp.h has the feature map and
+the exact arithmetic).  Runs under the proposal carry their log-likelihood
+ratio w.r.t. the nominal model, so ``flag * exp(logw)`` averages to the
+goal probability whatever the network; training only lowers the variance.
+
+CE training (multi-level, Rubinstein's method): each round simulates runs
+under the current proposal, takes as elite the runs whose tracked value
+reaches the round's level gamma = min(goal, (1-rho)-quantile of the tracked
+values), weights each elite run by its likelihood ratio, replays the elite
+runs on the GPU into training rows (four per step: features, a, b), and
+takes Adam steps on J = sum (b theta - a e^theta), the weighted
+log-likelihood of the elite paths under the proposal up to a constant; the
+gradient of J comes from the tensor-core kernel (csmc_mlp_grad).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._native import Query, Result, check, lib
+
+HID, IN = 64, 16
+GRAD_FLOATS = HID * IN + HID + HID * HID + HID + HID + 1
+ROW_BYTES = 40
+PARAM_BYTES = 11024
+THETA_MAX = 4.0
+
+
+def f32_to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    """Round to nearest even, as f_to_bf16 in csmc_mlp.h."""
+    b = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    nan = (b & 0x7FFFFFFF) > 0x7F800000
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint16)
+    r[nan] = ((b[nan] >> 16) | 0x40).astype(np.uint16)
+    return r
+
+
+def bf16_bits_to_f32(h: np.ndarray) -> np.ndarray:
+    return (np.asarray(h, dtype=np.uint32) << 16).view(np.float32)
+
+
+@dataclass
+class Proposal:
+    """FP32 master parameters; pack() gives the BF16 parameter block."""
+
+    w1: np.ndarray
+    b1: np.ndarray
+    w2: np.ndarray
+    b2: np.ndarray
+    w3: np.ndarray
+    b3: float = 0.0
+
+    @staticmethod
+    def init(seed: int = 0, scale: float = 1.0) -> "Proposal":
+        """He-style random hidden layers, zero output layer: theta = 0, the
+        proposal starts as the nominal model."""
+        rng = np.random.default_rng(seed)
+        w1 = (rng.standard_normal((HID, IN)) * math.sqrt(2.0 / 10) * scale).astype(np.float32)
+        w1[:, 10:] = 0.0
+        w2 = (rng.standard_normal((HID, HID)) * math.sqrt(2.0 / HID) * scale).astype(np.float32)
+        return Proposal(w1, np.zeros(HID, np.float32), w2, np.zeros(HID, np.float32), np.zeros(HID, np.float32), 0.0)
+
+    def vector(self) -> np.ndarray:
+        return np.concatenate([self.w1.ravel(), self.b1, self.w2.ravel(), self.b2, self.w3,
+                               np.array([self.b3], np.float32)]).astype(np.float32)
+
+    @staticmethod
+    def from_vector(v: np.ndarray) -> "Proposal":
+        v = np.asarray(v, dtype=np.float32)
+        o = 0
+        w1 = v[o:o + HID * IN].reshape(HID, IN).copy(); o += HID * IN
+        b1 = v[o:o + HID].copy(); o += HID
+        w2 = v[o:o + HID * HID].reshape(HID, HID).copy(); o += HID * HID
+        b2 = v[o:o + HID].copy(); o += HID
+        w3 = v[o:o + HID].copy(); o += HID
+        return Proposal(w1, b1, w2, b2, w3, float(v[o]))
+
+    def pack(self) -> bytes:
+        """csmc::MlpParams: w1 (BF16), b1, w2 (BF16), b2, w3, b3, pad."""
+        out = bytearray()
+        out += f32_to_bf16_bits(self.w1).tobytes()
+        out += np.asarray(self.b1, np.float32).tobytes()
+        out += f32_to_bf16_bits(self.w2).tobytes()
+        out += np.asarray(self.b2, np.float32).tobytes()
+        out += np.asarray(self.w3, np.float32).tobytes()
+        out += np.array([self.b3, 0, 0, 0], np.float32).tobytes()
+        assert len(out) == PARAM_BYTES
+        return bytes(out)
+
+
+class Adam:
+    def __init__(self, n: int, lr: float = 1e-2, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        self.m = np.zeros(n, np.float64)
+        self.v = np.zeros(n, np.float64)
+        self.t = 0
+        self.lr, self.b1, self.b2, self.eps = lr, b1, b2, eps
+
+    def ascend(self, x: np.ndarray, g: np.ndarray) -> np.ndarray:
+        self.t += 1
+        g = np.asarray(g, np.float64)
+        self.m = self.b1 * self.m + (1 - self.b1) * g
+        self.v = self.b2 * self.v + (1 - self.b2) * g * g
+        mh = self.m / (1 - self.b1 ** self.t)
+        vh = self.v / (1 - self.b2 ** self.t)
+        return (x + self.lr * mh / (np.sqrt(vh) + self.eps)).astype(np.float32)
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def is_run(net, query: Query, params: bytes, seed: int, n_runs: int, first_run: int = 0, flags=None, logw=None,
+           values=None, steps=None, stream=None) -> Result:
+    """csmc_is_run on a Network; per-run outputs are optional torch CUDA tensors."""
+    r = Result()
+    check(lib().csmc_is_run(net._h, ctypes.byref(query), params, seed & (2**64 - 1), first_run, n_runs,
+                            _ptr(flags), _ptr(logw), _ptr(values), _ptr(steps), ctypes.byref(r), stream))
+    return r
+
+
+def is_trace(net, query: Query, params: bytes, seed: int, runs, weights, row_offset, rows, first_run: int = 0,
+             stream=None) -> None:
+    """csmc_is_trace: runs/weights/row_offset/rows are torch CUDA tensors."""
+    check(lib().csmc_is_trace(net._h, ctypes.byref(query), params, seed & (2**64 - 1), first_run, _ptr(runs),
+                              _ptr(weights), _ptr(row_offset), len(runs), _ptr(rows), stream))
+
+
+def mlp_forward(params: bytes, rows, n_rows: int, theta, stream=None) -> None:
+    check(lib().csmc_mlp_forward(params, _ptr(rows), n_rows, _ptr(theta), stream))
+
+
+def mlp_grad(params: bytes, rows, n_rows: int, stream=None):
+    g = np.zeros(GRAD_FLOATS, np.float32)
+    J = ctypes.c_double()
+    check(lib().csmc_mlp_grad(params, _ptr(rows), n_rows, g.ctypes.data, ctypes.byref(J), stream))
+    return g, J.value
+
+
+@dataclass
+class TrainLog:
+    rounds: list = field(default_factory=list)
+
+
+def estimate(net, query: Query, proposal: Proposal | None, seed: int, n_runs: int, first_run: int = 0,
+             chunk: int = 2_000_000):
+    """Importance-sampling (or, with proposal None, plain) estimate of the
+    query's probability: (p, half-width of the 95% CI, device seconds)."""
+    import torch  # noqa: F401  (device buffers of the plain path)
+    s1 = s2 = 0.0
+    dev_s = 0.0
+    done = 0
+    params = (proposal or Proposal.init()).pack() if proposal is not None else None
+    while done < n_runs:
+        n = min(chunk, n_runs - done)
+        if proposal is None:
+            r = net.run(query, seed, n, first_run + done)
+            s1 += r.hits
+            s2 += r.hits
+        else:
+            r = is_run(net, query, params, seed, n, first_run + done)
+            s1 += r.sum
+            s2 += r.sum_sq
+        dev_s += r.kernel_ms / 1000.0
+        done += n
+    p = s1 / n_runs
+    var = max(s2 / n_runs - p * p, 0.0)
+    half = 1.96 * math.sqrt(var / n_runs)
+    return p, half, dev_s
+
+
+def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: int = 100_000, rho: float = 0.1,
+          adam_steps: int = 30, lr: float = 3e-3, init_seed: int = 0, max_rows: int = 40_000_000,
+          verbose: bool = False):
+    """CE training of the proposal on the GPU.  The goal is the query's
+    threshold event (tracked value > threshold for a max query).  Returns
+    (Proposal, TrainLog)."""
+    import torch
+    dev = torch.device("cuda")
+    prop = Proposal.init(init_seed)
+    x = prop.vector()
+    opt = Adam(x.size, lr=lr)
+    log = TrainLog()
+    n = runs_per_round
+    flags = torch.empty(n, dtype=torch.uint8, device=dev)
+    logw = torch.empty(n, dtype=torch.float64, device=dev)
+    values = torch.empty(n, dtype=torch.float64, device=dev)
+    steps = torch.empty(n, dtype=torch.int32, device=dev)
+    goal = query.threshold
+    for k in range(rounds):
+        t0 = time.perf_counter()
+        params = prop.pack()
+        first = (k + 1) * 10_000_000  # each round uses fresh runs of the stream
+        res = is_run(net, query, params, seed, n, first, flags=flags, logw=logw, values=values, steps=steps)
+        lw = logw.cpu().numpy()
+        val = values.cpu().numpy()
+        st = steps.cpu().numpy().view(np.uint32).astype(np.int64)
+        level = min(goal + 1e-9, float(np.quantile(val, 1.0 - rho)))
+        elite = np.nonzero(val >= level)[0] if level <= goal else np.nonzero(val > goal)[0]
+        if len(elite) == 0:
+            elite = np.argsort(val)[-max(1, int(rho * n)):]
+        w = np.exp(lw[elite] - lw[elite].max())
+        w = w / w.sum()
+        # cap the row set
+        order = np.argsort(-w)
+        rows_needed = 4 * st[elite]
+        keep = order[np.cumsum(rows_needed[order]) <= max_rows]
+        if len(keep) == 0:
+            keep = order[:1]
+        elite, w = elite[keep], w[keep]
+        w = (w / w.sum()).astype(np.float32)
+        offs = np.concatenate([[0], np.cumsum(4 * st[elite])[:-1]]).astype(np.uint64)
+        n_rows = int((4 * st[elite]).sum())
+        rows = torch.empty(n_rows * ROW_BYTES, dtype=torch.uint8, device=dev)
+        t_runs = torch.from_numpy(elite.astype(np.uint64).view(np.int64)).to(dev)
+        t_w = torch.from_numpy(w).to(dev)
+        t_off = torch.from_numpy(offs.view(np.int64)).to(dev)
+        is_trace(net, query, params, seed, t_runs, t_w, t_off, rows, first)
+        J0 = None
+        for _ in range(adam_steps):
+            g, J = mlp_grad(prop.pack(), rows, n_rows)
+            if J0 is None:
+                J0 = J
+            x = opt.ascend(x, g)
+            prop = Proposal.from_vector(x)
+        hit_est = float(res.estimate)
+        entry = {"round": k, "level": level, "elite": int(len(elite)), "rows": n_rows, "J_start": J0, "J_end": J,
+                 "estimate": hit_est, "hits": int(res.hits), "seconds": time.perf_counter() - t0}
+        log.rounds.append(entry)
+        if verbose:
+            print(entry, flush=True)
+        del rows
+    return prop, log

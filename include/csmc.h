@@ -72,7 +72,8 @@ typedef struct {
     int32_t lanes_per_run;  /* launch plan used: lanes per run (1: one thread per run) */
     int32_t comps_per_lane; /* components per lane */
     int32_t runs_per_cta;   /* runs in flight per CTA */
-    int32_t family;         /* 0 lane-group kernel, 1 thread-per-run kernel */
+    int32_t family;         /* 0 lane-group kernel, 1 thread-per-run kernel, 2 thread-per-run with
+                               the network in global memory (batch kernel, one job) */
 } csmc_result;
 
 /* Thread-local message of the last failure on this thread. */
@@ -136,10 +137,113 @@ int csmc_plan(const csmc_net *net, int32_t *lanes_per_run, int32_t *comps_per_la
 
 /* Overrides the launch plan of a network handle (used by the autotuner):
  * family 0 = lane groups of lanes_per_run lanes (power of two <= 32) with
- * comps_per_lane components each; family 1 = one thread per run (lanes and
+ * comps_per_lane components each; family 2 = one thread per run with the
+ * network and run state in global memory (networks larger than shared
+ * memory); family 1 = one thread per run (lanes and
  * comps_per_lane are ignored).  threads_per_cta: CTA size. */
 int csmc_set_plan(csmc_net *net, int32_t family, int32_t lanes_per_run, int32_t comps_per_lane,
                   int32_t threads_per_cta);
+
+/* Autotuner for one network (no counterpart in the reference, which has one
+ * fixed launch shape: one CTA per run, one thread per component).  Times
+ * csmc_run on runs 0 .. probe_runs-1 for every feasible plan — one thread
+ * per run at 64 and 128 threads per CTA, lane groups at 128 and 256 threads
+ * per CTA, and the global-memory plan at 64 and 128 — keeps the fastest on
+ * the handle and reports it in best (family, lanes_per_run, comps_per_lane,
+ * runs_per_cta, kernel_ms of its probe). */
+int csmc_autotune(csmc_net *net, const csmc_query *q, uint64_t seed, uint64_t probe_runs, csmc_result *best);
+
+/* ---- Batches: many (network, query) jobs in one persistent launch --------
+ * No counterpart in the reference, which simulates one model per process.
+ * Job j simulates the runs csmc_run(nets[j], &qs[j], seeds[j], first_runs[j],
+ * n_runs[j], ...) would simulate, with the same per-run results; all jobs'
+ * runs are drained from one device work queue by one persistent kernel, so
+ * small jobs and long runs do not leave the GPU idle the way a sequence of
+ * per-network launches does. */
+typedef struct csmc_batch csmc_batch;
+
+/* Builds a batch of n_jobs (1 .. 256) jobs on the current device.  first_runs
+ * may be NULL (all 0).  The network handles must outlive the batch.  verify
+ * != 0 also keeps per-run trace digests and final states (csmc_run_verify's
+ * outputs).  Allocates the per-run outputs, the job table, the run-state
+ * slabs and pinned host result buffers. */
+int csmc_batch_create(csmc_net *const *nets, const csmc_query *qs, const uint64_t *seeds, const uint64_t *first_runs,
+                      const uint64_t *n_runs, int32_t n_jobs, int32_t verify, csmc_batch **out);
+
+/* Launch geometry: threads per CTA (32..128, multiple of 32) and CTAs per SM
+ * (0: as many as fit). */
+int csmc_batch_set_plan(csmc_batch *b, int32_t threads_per_cta, int32_t ctas_per_sm);
+int csmc_batch_plan(const csmc_batch *b, int32_t *threads_per_cta, int32_t *ctas_per_sm);
+
+/* Enqueues the whole batch on stream — counter reset, the simulation, the
+ * per-job value sums and the copies of the counters and sums into the
+ * batch's pinned host buffers — without allocating or synchronising, so the
+ * sequence can be captured into a CUDA graph.  Read the results with
+ * csmc_batch_results after the stream has completed. */
+int csmc_batch_launch(csmc_batch *b, void *stream);
+
+/* Runs the batch and fills outs[0 .. n_jobs) in csmc_batch_create's job
+ * order.  use_graph != 0: the launch sequence is captured once into a CUDA
+ * graph (on a private stream) and the graph is replayed on stream.
+ * kernel_ms of every result is the device time of the whole batch. */
+int csmc_batch_run(csmc_batch *b, int32_t use_graph, void *stream, csmc_result *outs);
+
+/* Results of the last completed launch. */
+int csmc_batch_results(const csmc_batch *b, csmc_result *outs);
+
+/* Device per-run outputs of job j (run i of the job at index i; digests and
+ * final_state are NULL unless the batch verifies). */
+int csmc_batch_outputs(const csmc_batch *b, int32_t job, uint8_t **flags, double **values, uint32_t **steps,
+                       uint64_t **digests, uint32_t **final_state);
+
+/* The same outputs copied into host buffers (any may be NULL; synchronous). */
+int csmc_batch_outputs_host(const csmc_batch *b, int32_t job, uint8_t *flags, double *values, uint32_t *steps,
+                            uint64_t *digests, uint32_t *final_state);
+
+/* Autotuner for the batch: runs a probe batch (each job's runs scaled by
+ * probe_fraction, at least one run) at each candidate geometry (64 and 128
+ * threads per CTA, every CTAs-per-SM count that fits), keeps the fastest, and
+ * orders the jobs in the run space by measured cost per run, most expensive
+ * first, so that the cheapest runs fill the end of the batch. */
+int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_per_cta, int32_t *ctas_per_sm);
+
+void csmc_batch_free(csmc_batch *b);
+
+/* ---- Importance sampling with a learned proposal ------------------------
+ * No counterpart in the reference.  The proposal network (16 -> 64 -> 64 ->
+ * 1, GELU, BF16 weights) tilts every exponential rate by exp(theta); the
+ * parameter block layout is csmc::MlpParams of cusmc_b200/csrc/include/
+ * csmc_mlp.h (CSMC_MLP_PARAM_BYTES bytes). */
+#define CSMC_MLP_PARAM_BYTES 11024
+
+/* Runs first_run .. first_run+n_runs-1 under the proposal.  Per-run device
+ * outputs (may be NULL): flags, logw (log-likelihood ratio nominal/proposal,
+ * FP64), values (tracked max/min), steps.  out->sum / sum_sq are the sums of
+ * flag * exp(logw) and of its square; out->estimate = sum / n_runs is the
+ * unbiased importance-sampling estimate of the query's probability. */
+int csmc_is_run(csmc_net *net, const csmc_query *q, const void *params, uint64_t seed, uint64_t first_run,
+                uint64_t n_runs, uint8_t *flags, double *logw, double *values, uint32_t *steps, csmc_result *out,
+                void *stream);
+
+/* Replays runs first_run + runs[i] (device list of n_list offsets) under the
+ * proposal and writes their CE training rows (csmc::MlpRow, 40 bytes: BF16
+ * features, a, b) to rows: four rows per step starting at row_offset[i]
+ * (device), weighted by weights[i] (device). */
+int csmc_is_trace(csmc_net *net, const csmc_query *q, const void *params, uint64_t seed, uint64_t first_run,
+                  const uint64_t *runs, const float *weights, const uint64_t *row_offset, uint64_t n_list, void *rows,
+                  void *stream);
+
+/* Tensor-core (tcgen05) forward pass of the proposal network over n_rows
+ * device rows (csmc::MlpRow): theta (device, n_rows floats, clipped). */
+int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, float *theta, void *stream);
+
+/* Tensor-core gradient of J = sum over rows of (b theta - a e^theta) with
+ * respect to the parameters (host floats, CSMC_MLP_GRAD_FLOATS of them:
+ * w1[64][16], b1[64], w2[64][64], b2[64], w3[64], b3); *objective = J.
+ * BF16 operands, FP32 accumulation in tensor memory. */
+#define CSMC_MLP_GRAD_FLOATS 5313
+int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
+                  void *stream);
 
 /* Scratch bytes per device behind csmc_run_noalloc (held from the first
  * call on a device until the process exits). */

@@ -29,6 +29,7 @@
 #include "../include/csmc.h"
 #include "../cusmc_b200/csrc/include/csmc_net.h"
 #include "../cusmc_b200/csrc/include/csmc_numeric.h"
+#include "../cusmc_b200/csrc/include/csmc_mlp.h"
 
 #include <algorithm>
 #include <atomic>
@@ -197,6 +198,38 @@ class Run {
         return exp_delay(x, inv_rate(eval(L.rate)));
     }
 
+    // The delay under the importance-sampling proposal: exponential delays
+    // of finite positive 1/rate are drawn with 1/rate multiplied by the
+    // component's class factor e^(-theta).
+    float delay_is(uint32_t c, const float *mfac, bool &tilted, float &inv, float &invp) const {
+        tilted = false;
+        inv = invp = 0.0f;
+        const csmc_loc &L = n_.loc[n_.comp[c].loc_begin + loc_[c]];
+        if (L.type > 1) return 0.0f;
+        double max_delay = kDblMax;
+        bool bounded = false;
+        for (uint32_t i = 0; i < L.n_inv; ++i) {
+            const csmc_guard &g = n_.guard[L.inv_begin + i];
+            const double cur = static_cast<double>(vars_[g.var]);
+            const double bound = eval(g.rhs);
+            double ttb = bound - cur;
+            if (g.op == CSMC_G_LT) ttb -= 1e-6;
+            if (ttb >= 0) {
+                max_delay = std::fmin(max_delay, ttb);
+                bounded = true;
+            }
+        }
+        const uint32_t x = delay_word(seed_, run_, step_, c);
+        if (bounded) return uniform_delay(x, max_delay);
+        inv = inv_rate(eval(L.rate));
+        invp = inv;
+        if (tiltable(inv)) {
+            invp = f_mul(inv, mfac[loc_[c] & 3u]);
+            tilted = true;
+        }
+        return exp_delay(x, invp);
+    }
+
     // simulation.cu:9-24 and 27-181.  en: enabled edge indices (ascending).
     void take(uint32_t c, const std::vector<uint32_t> &en, uint32_t choice_which) {
         const uint32_t n = static_cast<uint32_t>(en.size());
@@ -269,10 +302,11 @@ class Run {
         if (q_.var_id >= 0 && static_cast<uint32_t>(q_.var_id) < V && n_.var[q_.var_id].kind == 0)
             qmin_ = qmax_ = static_cast<double>(n_.var[q_.var_id].init);
         const float T = static_cast<float>(q_.horizon);
-        const uint64_t cap = q_.max_steps ? q_.max_steps : 0xffffffffull;
+        const uint64_t cap = q_.max_steps ? q_.max_steps : 10000000ull;
         const bool loc_mode = q_.kind == CSMC_QUERY_LOCATION;
         const uint32_t bits = ceil_log2(C);
-        std::vector<float> d(C);
+        std::vector<float> d(C), inv(C), invp(C);
+        std::vector<uint8_t> tilted(C);
         std::vector<uint32_t> keys(C), idx(C);
         std::vector<std::vector<uint32_t>> recv(C);
         std::vector<uint32_t> en;
@@ -306,8 +340,24 @@ class Run {
                 chan_ = 0;
                 sender_ = -1;
             }
+            float mfac[CSMC_MLP_CLASSES] = {1.0f, 1.0f, 1.0f, 1.0f};
+            float feat[CSMC_MLP_CLASSES][CSMC_MLP_IN];
+            if (mlp_) {  // the proposal's class factors for this step
+                float v4[4] = {0, 0, 0, 0};
+                for (uint32_t i = 0; i < 4 && i < V; ++i) v4[i] = vars_[i];
+                for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) {
+                    mlp_features(l, v4, V < 4 ? V : 4, C, time, T, feat[l]);
+                    mfac[l] = tilt_factor(mlp_theta(*mlp_, feat[l]));
+                }
+            }
             for (uint32_t c = 0; c < C; ++c) {
-                d[c] = delay(c);
+                if (mlp_) {
+                    bool t = false;
+                    d[c] = delay_is(c, mfac, t, inv[c], invp[c]);
+                    tilted[c] = t;
+                } else {
+                    d[c] = delay(c);
+                }
                 keys[c] = delay_key(d[c]);
                 idx[c] = c;
             }
@@ -323,6 +373,30 @@ class Run {
                 }
             const uint32_t win = idx[0];
             const float dmin = d[win];
+            const bool finite = static_cast<double>(dmin) < kDblMax;
+            if (mlp_ && finite) {
+                double sum = 0.0;
+                for (uint32_t c = 0; c < C; ++c)
+                    if (tilted[c]) sum = d_add(sum, rate_change(inv[c], invp[c]));
+                logw_ = d_add(logw_, step_log_ratio(sum, dmin, tilted[win] != 0, inv[win], invp[win]));
+            }
+            if (mlp_ && rows_) {  // four rows per step, zero-weighted where nothing is tilted
+                for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) {
+                    double inv_sum = 0.0;
+                    uint32_t count = 0;
+                    for (uint32_t c = 0; c < C; ++c)
+                        if (tilted[c] && (loc_[c] & 3u) == l) {
+                            inv_sum = d_add(inv_sum, d_div(1.0, static_cast<double>(inv[c])));
+                            ++count;
+                        }
+                    const bool has = finite && count > 0;
+                    MlpRow r;
+                    for (int i = 0; i < CSMC_MLP_IN; ++i) r.x[i] = f_to_bf16(feat[l][i]);
+                    r.a = has ? row_a(inv_sum, dmin, row_w_) : 0.0f;
+                    r.b = (has && tilted[win] && (loc_[win] & 3u) == l) ? row_w_ : 0.0f;
+                    rows_->push_back(r);
+                }
+            }
             if (digest_) {
                 dg_.mix(step_);
                 dg_.mix(win);
@@ -347,6 +421,10 @@ class Run {
         time_ = time;
     }
 
+    const MlpParams *mlp_ = nullptr;   // importance sampling: the proposal network
+    double logw_ = 0.0;                 // log-likelihood ratio of the path
+    std::vector<MlpRow> *rows_ = nullptr;  // replay: training rows
+    float row_w_ = 0.0f;                // replay: the run's CE weight
     uint8_t flag_ = 0;
     bool capped_ = false;
     uint32_t step_ = 0;
@@ -486,6 +564,145 @@ int oracle_trace(const void *blob, size_t bytes, const csmc_query *q, uint64_t s
         g_err = e.what();
         return CSMC_ERR_ARG;
     }
+}
+
+/* Importance sampling under the proposal network P (host MlpParams):
+ * per run (host, may be NULL): flags, log-likelihood ratios (nominal over
+ * proposal), tracked values, steps.  Threads as oracle_run. */
+int oracle_is_run(const void *blob, size_t bytes, const csmc_query *q, const void *params, uint64_t seed,
+                  uint64_t first_run, uint64_t n_runs, int threads, uint8_t *flags, double *logw, double *values,
+                  uint32_t *steps, double *wall_ms) {
+    try {
+        if (!q || !params) throw std::runtime_error("null argument");
+        const Net n = view(blob, bytes);
+        const MlpParams *P = static_cast<const MlpParams *>(params);
+        int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+        if (nt < 1) nt = 1;
+        if (static_cast<uint64_t>(nt) > n_runs) nt = static_cast<int>(std::max<uint64_t>(1, n_runs));
+        std::atomic<uint64_t> next{0};
+        auto worker = [&]() {
+            for (;;) {
+                const uint64_t i = next.fetch_add(1);
+                if (i >= n_runs) break;
+                Run r(n, *q, seed, first_run + i);
+                r.mlp_ = P;
+                r.simulate(false);
+                const double val = q->is_max ? r.qmax_ : r.qmin_;
+                uint8_t f = r.flag_;
+                if (q->kind == CSMC_QUERY_VARIABLE) f = q->is_max ? (val > q->threshold) : (val < q->threshold);
+                if (flags) flags[i] = f;
+                if (logw) logw[i] = r.logw_;
+                if (values) values[i] = val;
+                if (steps) steps[i] = r.step_;
+            }
+        };
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto &th : pool) th.join();
+        if (wall_ms)
+            *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return CSMC_ERR_ARG;
+    }
+}
+
+/* Replays runs first_run + runs[i] under P and appends their training rows
+ * (weighted by weights[i]) in run-list order to rows (capacity cap rows);
+ * *n_rows receives the number written (CSMC_ERR_LIMIT when cap is short). */
+int oracle_is_trace(const void *blob, size_t bytes, const csmc_query *q, const void *params, uint64_t seed,
+                    uint64_t first_run, const uint64_t *runs, const float *weights, uint64_t n_list, void *rows,
+                    uint64_t cap, uint64_t *n_rows) {
+    try {
+        const Net n = view(blob, bytes);
+        const MlpParams *P = static_cast<const MlpParams *>(params);
+        std::vector<MlpRow> out;
+        for (uint64_t i = 0; i < n_list; ++i) {
+            Run r(n, *q, seed, first_run + runs[i]);
+            r.mlp_ = P;
+            r.rows_ = &out;
+            r.row_w_ = weights[i];
+            r.simulate(false);
+        }
+        *n_rows = out.size();
+        if (out.size() > cap) {
+            g_err = "row buffer too small";
+            return CSMC_ERR_LIMIT;
+        }
+        std::memcpy(rows, out.data(), out.size() * sizeof(MlpRow));
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return CSMC_ERR_ARG;
+    }
+}
+
+/* theta of one feature row (16 floats). */
+float oracle_mlp_theta(const void *params, const float *x) {
+    return mlp_theta(*static_cast<const MlpParams *>(params), x);
+}
+
+/* Gradient of J = sum over rows of (b theta - a e^theta) with respect to the
+ * network's parameters, with the tensor-core kernels' roundings (first-layer
+ * activations and the back-propagated pre-activation gradients in BF16),
+ * accumulated in double.  grad (floats): w1[64][16], b1[64], w2[64][64],
+ * b2[64], w3[64], b3.  objective receives J. */
+int oracle_mlp_grad(const void *params, const void *rows_v, uint64_t n_rows, float *grad, double *objective) {
+    const MlpParams &P = *static_cast<const MlpParams *>(params);
+    const MlpRow *rows = static_cast<const MlpRow *>(rows_v);
+    constexpr int H = CSMC_MLP_HID, I = CSMC_MLP_IN;
+    std::vector<double> gw1(H * I, 0.0), gb1(H, 0.0), gw2(H * H, 0.0), gb2(H, 0.0), gw3(H, 0.0);
+    double gb3 = 0.0, J = 0.0;
+    float x[I], z1[H], h1[H], z2[H], h2[H], dz2b[H], dz1b[H];
+    for (uint64_t r = 0; r < n_rows; ++r) {
+        for (int i = 0; i < I; ++i) x[i] = bf16_to_f(rows[r].x[i]);
+        for (int j = 0; j < H; ++j) {
+            float z = P.b1[j];
+            for (int i = 0; i < I; ++i) z = f_fma(x[i], bf16_to_f(P.w1[j][i]), z);
+            z1[j] = z;
+            h1[j] = bf16_round(gelu_f(z));
+        }
+        float th = P.b3;
+        for (int k = 0; k < H; ++k) {
+            float z = P.b2[k];
+            for (int j = 0; j < H; ++j) z = f_fma(h1[j], bf16_to_f(P.w2[k][j]), z);
+            z2[k] = z;
+            h2[k] = gelu_f(z);
+            th = f_fma(h2[k], P.w3[k], th);
+        }
+        const bool inside = th >= -CSMC_MLP_THETA_MAX && th <= CSMC_MLP_THETA_MAX;
+        const float thc = inside ? th : (th < 0 ? -CSMC_MLP_THETA_MAX : CSMC_MLP_THETA_MAX);
+        const float e = exp2_f(f_mul(thc, 1.44269502f));
+        J += static_cast<double>(rows[r].b) * thc - static_cast<double>(rows[r].a) * e;
+        const float g = inside ? f_add(rows[r].b, -f_mul(rows[r].a, e)) : 0.0f;
+        if (g == 0.0f) continue;
+        gb3 += g;
+        for (int k = 0; k < H; ++k) {
+            gw3[k] += static_cast<double>(g) * h2[k];
+            dz2b[k] = bf16_round(f_mul(f_mul(g, P.w3[k]), gelu_grad_f(z2[k])));
+            gb2[k] += dz2b[k];
+            for (int j = 0; j < H; ++j) gw2[k * H + j] += static_cast<double>(dz2b[k]) * h1[j];
+        }
+        for (int j = 0; j < H; ++j) {
+            double dh = 0.0;
+            for (int k = 0; k < H; ++k) dh += static_cast<double>(dz2b[k]) * bf16_to_f(P.w2[k][j]);
+            dz1b[j] = bf16_round(f_mul(static_cast<float>(dh), gelu_grad_f(z1[j])));
+            gb1[j] += dz1b[j];
+            for (int i = 0; i < I; ++i) gw1[j * I + i] += static_cast<double>(dz1b[j]) * x[i];
+        }
+    }
+    float *o = grad;
+    for (double v : gw1) *o++ = static_cast<float>(v);
+    for (double v : gb1) *o++ = static_cast<float>(v);
+    for (double v : gw2) *o++ = static_cast<float>(v);
+    for (double v : gb2) *o++ = static_cast<float>(v);
+    for (double v : gw3) *o++ = static_cast<float>(v);
+    *o = static_cast<float>(gb3);
+    if (objective) *objective = J;
+    return CSMC_OK;
 }
 
 }  // extern "C"

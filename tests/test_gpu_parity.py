@@ -34,7 +34,7 @@ def _lane_shape(n_comps):
 
 def _compare(blob, query, seed, n_runs, first_run=0, family=None):
     """family None: the library's default plan; 0: lane groups; 1: one
-    thread per run."""
+    thread per run; 2: one thread per run, network in global memory."""
     import oracle
     net = api.Network(blob)
     try:
@@ -43,6 +43,8 @@ def _compare(blob, query, seed, n_runs, first_run=0, family=None):
             net.set_plan(0, g, k, 256)
         elif family == 1:
             net.set_plan(1, 1, 1, 128)
+        elif family == 2:
+            net.set_plan(2, 1, 1, 128)
         r_dev, dev = net.run_verify(query, seed, n_runs, first_run)
     finally:
         net.close()
@@ -71,7 +73,24 @@ def _fixture_nets():
 FIXTURE_CASES = [(m["name"], m["mode"]) for m in _fixture_nets() if m["name"] != "CSMA_100"]
 
 
-@pytest.mark.parametrize("family", [0, 1])
+@pytest.mark.parametrize("mode", ["loc", "var"])
+def test_network_larger_than_shared_memory(mode):
+    """CSMA_100's packed network does not fit in shared memory: the default
+    plan reads it from global memory (family 2)."""
+    with open(os.path.join(GOLDEN, "nets", f"CSMA_100.{mode}.blob"), "rb") as f:
+        blob = f.read()
+    assert len(blob) > 227 * 1024
+    info = api.blob_info(blob)
+    if mode == "loc":
+        q = api.location_query(horizon=100, max_steps=20_000)
+    else:
+        q = api.variable_query(var_id=min(1, info["n_vars"] - 1), horizon=100, threshold=0, is_max=True,
+                               max_steps=20_000)
+    r_dev, _ = _compare(blob, q, seed=1235, n_runs=64)
+    assert r_dev.family == 2
+
+
+@pytest.mark.parametrize("family", [0, 1, 2])
 @pytest.mark.parametrize("name,mode", FIXTURE_CASES)
 def test_reference_fixtures(name, mode, family):
     with open(os.path.join(GOLDEN, "nets", f"{name}.{mode}.blob"), "rb") as f:
@@ -101,7 +120,7 @@ def _blob(w, loc=False):
         os.unlink(path)
 
 
-@pytest.mark.parametrize("family", [0, 1])
+@pytest.mark.parametrize("family", [0, 1, 2])
 def test_epidemic_1000_runs(family):
     w = netgen.epidemic()
     blob = _blob(w)
@@ -109,7 +128,7 @@ def test_epidemic_1000_runs(family):
     _compare(blob, q, seed=2024, n_runs=1000, family=family)
 
 
-@pytest.mark.parametrize("family", [0, 1])
+@pytest.mark.parametrize("family", [0, 1, 2])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
 def test_random_networks(seed, family):
     w = netgen.random_network(seed)
@@ -118,7 +137,7 @@ def test_random_networks(seed, family):
     _compare(blob, q, seed=7 + seed, n_runs=2000, family=family)
 
 
-@pytest.mark.parametrize("family", [0, 1])
+@pytest.mark.parametrize("family", [0, 1, 2])
 @pytest.mark.parametrize("n", [8, 32])
 def test_mutex(n, family):
     w = netgen.mutex(n)
