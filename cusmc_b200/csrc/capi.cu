@@ -211,8 +211,8 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     int ctas = 0;
     int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
              : n->family == 2 ? csmc::batch_max_active_ctas(verify, n->block, n->smem, &ctas)
-                              : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->block,
-                                                             n->smem, &ctas);
+                              : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->classes,
+                                                             n->block, n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network (shared memory)");
     int sms = 0;
@@ -272,7 +272,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     rc = n->family == 0   ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block,
                                              n->smem, st)
          : n->family == 2 ? csmc::batch_launch(verify, bp, static_cast<int>(grid), n->block, st)
-                          : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, p,
+                          : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, n->classes, p,
                                                 static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
@@ -423,6 +423,7 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     n->bytes = (h->total_bytes + 15u) & ~15u;
     n->slots = h->max_edges_per_loc >= 2;
     n->loc8 = h->max_locs_per_comp <= 256;
+    n->classes = (h->flags & CSMC_NET_RACE_CLASSES) != 0 && h->n_comps <= 256;
     // default plan: one thread per run when the run state of a 128-thread
     // CTA fits next to the network in shared memory, lane groups otherwise
     std::string why;

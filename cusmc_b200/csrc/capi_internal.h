@@ -29,7 +29,8 @@ struct csmc_net {
     size_t smem = 0;
     uint32_t state_stride = 0;
     bool slots = false;
-    bool loc8 = false;  // every automaton has at most 256 locations
+    bool loc8 = false;     // every automaton has at most 256 locations
+    bool classes = false;  // delay descriptors carry race classes
     bool state_in_global = false;
     uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
     size_t state_bytes = 0;

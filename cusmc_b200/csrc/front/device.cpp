@@ -20,6 +20,7 @@
 #include <map>
 #include <set>
 #include <stdexcept>
+#include <limits>
 #include <unordered_set>
 
 namespace csmc {
@@ -702,6 +703,29 @@ class Packer {
                 std::memcpy(&lo, &inv_lit[slot], 4);
             }
             loc_desc.push_back(static_cast<uint64_t>(lo) | (static_cast<uint64_t>(flags) << 32));
+        }
+        // race classes: always-exponential locations sharing the source of
+        // their 1/rate (a literal of finite positive value, or one per-step
+        // rate program)
+        {
+            std::map<uint64_t, uint32_t> cls;
+            bool ok = comps_.size() <= 256;
+            for (uint64_t &d : loc_desc) {
+                const uint32_t fl = static_cast<uint32_t>(d >> 32), lo = static_cast<uint32_t>(d);
+                float inv;
+                std::memcpy(&inv, &lo, 4);
+                const bool lit_ok = (fl & CSMC_DESC_PROG) || (inv > 0.0f && inv <= std::numeric_limits<float>::max());
+                uint32_t c = CSMC_DESC_NO_CLASS;
+                if (!(fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL)) && lit_ok) {
+                    const uint64_t key = d & (0xffffffffull | (static_cast<uint64_t>(CSMC_DESC_PROG) << 32));
+                    auto it = cls.find(key);
+                    if (it == cls.end()) it = cls.emplace(key, static_cast<uint32_t>(cls.size())).first;
+                    if (it->second >= CSMC_RACE_CLASSES) ok = false;
+                    c = it->second & 0xffu;
+                }
+                d |= static_cast<uint64_t>(c << 8) << 32;
+            }
+            if (ok && !cls.empty()) h.flags |= CSMC_NET_RACE_CLASSES;
         }
         h.magic = CSMC_NET_MAGIC;
         h.version = CSMC_NET_VERSION;

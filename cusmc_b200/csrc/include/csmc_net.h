@@ -89,7 +89,8 @@ typedef struct {
 } csmc_net_header; /* 160 bytes */
 
 /* Header flags. */
-#define CSMC_NET_RATE_TABLE 1u /* rates resolved through loc_rate (see below) */
+#define CSMC_NET_RATE_TABLE 1u  /* rates resolved through loc_rate (see below) */
+#define CSMC_NET_RACE_CLASSES 2u /* delay descriptors carry race classes (see below) */
 
 /* Rate slot of a location (loc_rate[]): bit 15 set -> index into the
  * per-step table of evaluated rate programs (rate_prog[]); clear -> index
@@ -106,6 +107,15 @@ typedef struct {
 #define CSMC_DESC_ZERO (1u << 1)  /* branch / urgent / committed: delay 0 */
 #define CSMC_DESC_INV (1u << 2)   /* has delay-bounding invariants */
 #define CSMC_DESC_EVAL (1u << 3)  /* rate evaluated per component (no table) */
+/* Race class (high word bits 8..15; 0xff: none): locations whose delay is
+ * always exponential with 1/rate from the same literal or the same per-step
+ * rate program.  Within a class the delay is a non-increasing function of
+ * the 24-bit uniform draw, so the race only needs each class's largest draws
+ * (set, with CSMC_NET_RACE_CLASSES, when a network has at most
+ * CSMC_RACE_CLASSES classes and at most 256 components). */
+#define CSMC_DESC_CLASS(fl) (((fl) >> 8) & 0xffu)
+#define CSMC_DESC_NO_CLASS 0xffu
+#define CSMC_RACE_CLASSES 4
 
 typedef struct {
     uint32_t loc_begin;  /* global index of the component's first location */

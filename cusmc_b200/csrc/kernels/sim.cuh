@@ -80,9 +80,11 @@ bool sim_supported(int lanes_per_run, int comps_per_lane);
 // several edges, so enabled-edge slot masks are kept):
 // loc8: locations kept as 8-bit local indices (every automaton has at most
 // 256 locations); gstate: run state in global slabs instead of shared memory.
-int serial_launch(bool verify, bool slots, bool loc8, bool gstate, const SimParams &p, int grid, int block,
-                  size_t smem, void *stream);
-int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, int block, size_t smem, int *ctas);
+// classes: the network's delay descriptors carry race classes.
+int serial_launch(bool verify, bool slots, bool loc8, bool gstate, bool classes, const SimParams &p, int grid,
+                  int block, size_t smem, void *stream);
+int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, bool classes, int block, size_t smem,
+                           int *ctas);
 
 // ---- Multi-network batch kernel (sim_batch.cuh) ---------------------------
 // One persistent launch simulates the runs of many (network, query) jobs.
@@ -131,7 +133,7 @@ int batch_max_active_ctas(bool verify, int block, size_t smem, int *ctas);
 inline size_t batch_smem_bytes(uint32_t n_jobs) { return static_cast<size_t>(n_jobs) * sizeof(BatchJob); }
 // Bytes of one thread's state in a batch slab (16-bit locations, slot masks).
 inline size_t batch_state_bytes_per_thread(uint32_t max_comps, uint32_t max_vars, uint32_t max_rate_prog) {
-    return 4u * (2u * max_vars + max_rate_prog) + 2u * max_comps + 4u * max_comps + 4u;
+    return 4u * (2u * max_vars + max_rate_prog + 2u * CSMC_RACE_CLASSES) + 2u * max_comps + 4u * max_comps + 4u;
 }
 
 // ---- Importance sampling (sim_is.cuh) --------------------------------------
@@ -164,6 +166,7 @@ int mlp_tc_partial_floats();
 inline size_t serial_state_bytes_per_thread(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots,
                                             bool loc8) {
     size_t b = 4u * (2u * n_vars + n_rate_prog);        // variables, rate table, receiver snapshot
+    b += 4u * 2u * CSMC_RACE_CLASSES;                   // race-class keys
     b += loc8 ? ((n_comps + 3u) & ~3u) : ((2u * n_comps + 3u) & ~3u);  // locations
     if (slots) b += 4u * n_comps;                       // enabled-edge slot masks
     return b;

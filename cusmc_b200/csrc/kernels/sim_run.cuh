@@ -40,6 +40,7 @@ struct RunView {
     VarView vars, rates, shadow;
     LocT *locs;       // this thread's element 0; stride T
     uint32_t *slotv;  // this thread's element 0; stride T
+    uint32_t *cls;    // race-class keys: [g] largest, [4 + g] second largest; stride T
     uint32_t T;
 
     // global location index of component c
@@ -58,7 +59,8 @@ static __host__ __device__ __forceinline__ uint32_t run_loc_bytes(uint32_t C, ui
 }
 
 // Carves thread t's views out of a state slab of T threads laid out as
-// vars[V] | rates[P] | shadow[V] (floats) | locs[C] | slots[C] (u32).
+// vars[V] | rates[P] | shadow[V] (floats) | race-class keys[8] | locs[C] |
+// slots[C] (u32).
 template <bool LOC8>
 static __device__ __forceinline__ RunView<LOC8> carve_run_view(uint8_t *st, uint32_t V, uint32_t P, uint32_t C,
                                                                  uint32_t T, uint32_t t) {
@@ -68,8 +70,10 @@ static __device__ __forceinline__ RunView<LOC8> carve_run_view(uint8_t *st, uint
     r.vars = VarView{fb + t, T};
     r.rates = VarView{fb + V * T + t, T};
     r.shadow = VarView{fb + (V + P) * T + t, T};
-    r.locs = reinterpret_cast<LocT *>(st + 4u * (2u * V + P) * T) + t;
-    r.slotv = reinterpret_cast<uint32_t *>(st + 4u * (2u * V + P) * T + run_loc_bytes(C, T, LOC8)) + t;
+    r.cls = reinterpret_cast<uint32_t *>(st + 4u * (2u * V + P) * T) + t;
+    const uint32_t lb = 4u * (2u * V + P + 2u * CSMC_RACE_CLASSES) * T;
+    r.locs = reinterpret_cast<LocT *>(st + lb) + t;
+    r.slotv = reinterpret_cast<uint32_t *>(st + lb + run_loc_bytes(C, T, LOC8)) + t;
     r.T = T;
     return r;
 }
@@ -189,24 +193,14 @@ static __device__ __forceinline__ void run_commit(const Net &n, uint32_t n_clock
     ++step;
 }
 
-// One step of a run: pending broadcast receivers, the per-step rate table,
-// the race, the clock advance and the winner's transition, the time update.
-template <bool VERIFY, bool SLOTS, bool LOC8>
-static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32_t V, uint32_t P, uint32_t n_clocks,
-                                                bool rate_table, const RunView<LOC8> &rv, RunScalars &sc,
-                                                uint64_t seed, int var_id, uint64_t run, uint32_t &step,
-                                                float &time) {
-    const uint32_t bits = ceil_log2(C);
-    const VarView vars = rv.vars, rates = rv.rates;
-    run_receivers<VERIFY, SLOTS, LOC8>(n, C, V, rv, sc, seed, var_id, run, step);
-
-    // ---- distinct rate programs, once per step
-    if (rate_table)
-        for (uint32_t j = 0; j < P; ++j) rates[j] = inv_rate(eval(n, vars, n.rate_prog[j]));
-
-    // ---- delays and the race (simulation.cu:409-628)
-    unsigned long long best = ~0ull;
-    float bestd = 0.0f;
+// The race over every component (simulation.cu:409-628): per-component
+// delays, minimum of (delay key, bit-reversed index).
+template <bool LOC8>
+static __device__ __forceinline__ void race_exact(const Net &n, uint32_t C, uint32_t bits, const RunView<LOC8> &rv,
+                                                  uint64_t seed, uint64_t run, uint32_t step, unsigned long long &best,
+                                                  float &bestd) {
+    best = ~0ull;
+    bestd = 0.0f;
     for (uint32_t c = 0; c < C; c += 4) {
         const u32x4 blk = delay_block(seed, run, step, c >> 2);
 #pragma unroll
@@ -222,10 +216,10 @@ static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32
                 const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
                 const uint32_t x = word_of(blk, k);
                 float inv = __uint_as_float(lo);
-                if (fl & CSMC_DESC_PROG) inv = rates[lo];
+                if (fl & CSMC_DESC_PROG) inv = rv.rates[lo];
                 float d = exp_delay(x, inv);
                 if (fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL))
-                    d = (fl & CSMC_DESC_ZERO) ? 0.0f : slow_delay(n, vars, rates, li, x);
+                    d = (fl & CSMC_DESC_ZERO) ? 0.0f : slow_delay(n, rv.vars, rv.rates, li, x);
                 const unsigned long long key =
                     (static_cast<unsigned long long>(delay_key(d)) << 32) | bitrev_bits(cc, bits);
                 if (key < best) {
@@ -234,6 +228,128 @@ static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32
                 }
             }
         }
+    }
+}
+
+// The same race decided from race classes: within a class the delay is a
+// non-increasing function of the 24-bit uniform draw m (log2 of the draw is
+// monotone over all 2^24 draws, and multiplying by a positive 1/rate keeps
+// the order), so a class is represented by its largest key (m, then the
+// smallest bit-reversed index) and needs no logarithm per member.  Two
+// members of a class tie only when their draws give the same float delay;
+// when that cannot be ruled out from the two largest keys (or when a class's
+// 1/rate is not finite and positive and the class could take part in the
+// minimum) the function returns false and the caller runs race_exact.
+template <bool LOC8>
+static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, uint32_t bits, const RunView<LOC8> &rv,
+                                                    uint64_t seed, uint64_t run, uint32_t step,
+                                                    unsigned long long &best, float &bestd) {
+    const uint32_t T = rv.T;
+    uint32_t pres = 0, pres2 = 0;
+    best = ~0ull;
+    bestd = 0.0f;
+    for (uint32_t c = 0; c < C; c += 4) {
+        const u32x4 blk = delay_block(seed, run, step, c >> 2);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t cc = c + k;
+            if (cc < C) {
+                const uint32_t li = rv.loc(n, cc);
+                const uint64_t dsc = n.loc_desc[li];
+                const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
+                const uint32_t x = word_of(blk, k);
+                const uint32_t br = bitrev_bits(cc, bits);
+                const uint32_t g = CSMC_DESC_CLASS(fl);
+                if (g < CSMC_RACE_CLASSES) {
+                    const uint32_t key = (x & 0xffffff00u) | (255u - br);
+                    const uint32_t bit = 1u << g;
+                    uint32_t *k1 = rv.cls + g * T, *k2 = rv.cls + (CSMC_RACE_CLASSES + g) * T;
+                    if (!(pres & bit)) {
+                        *k1 = key;
+                        pres |= bit;
+                    } else {
+                        const uint32_t a = *k1;
+                        if (key > a) {
+                            *k1 = key;
+                            *k2 = a;
+                        } else if (!(pres2 & bit) || key > *k2) {
+                            *k2 = key;
+                        }
+                        pres2 |= bit;
+                    }
+                } else {
+                    float d;
+                    if (fl & CSMC_DESC_ZERO) {
+                        d = 0.0f;
+                    } else if (fl & (CSMC_DESC_INV | CSMC_DESC_EVAL)) {
+                        d = slow_delay(n, rv.vars, rv.rates, li, x);
+                    } else {
+                        const float inv = (fl & CSMC_DESC_PROG) ? rv.rates[lo] : __uint_as_float(lo);
+                        d = exp_delay(x, inv);
+                    }
+                    const unsigned long long key = (static_cast<unsigned long long>(delay_key(d)) << 32) | br;
+                    if (key < best) {
+                        best = key;
+                        bestd = d;
+                    }
+                }
+            }
+        }
+    }
+    uint32_t inf_classes = 0;
+#pragma unroll
+    for (uint32_t g = 0; g < CSMC_RACE_CLASSES; ++g) {
+        const uint32_t bit = 1u << g;
+        if (!(pres & bit)) continue;
+        const uint32_t a = rv.cls[g * T];
+        const uint32_t m1 = a >> 8, br1 = 255u - (a & 255u);
+        const uint32_t li = rv.loc(n, bitrev_bits(br1, bits));
+        const uint64_t dsc = n.loc_desc[li];
+        const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
+        const float inv = (fl & CSMC_DESC_PROG) ? rv.rates[lo] : __uint_as_float(lo);
+        if (!(inv > 0.0f)) return false;  // delays 0, negative or NaN for the whole class
+        if (!(inv <= 3.40282347e38f)) {   // +inf: the class's delays are +inf (NaN at u = 1)
+            inf_classes |= bit;
+            continue;
+        }
+        const float d1 = exp_delay(m1 << 8, inv);
+        if (m1 > 0 && (pres2 & bit) && exp_delay((m1 - 1u) << 8, inv) == d1) {
+            const uint32_t m2 = rv.cls[(CSMC_RACE_CLASSES + g) * T] >> 8;
+            if (m2 == m1 || exp_delay(m2 << 8, inv) == d1) return false;
+        }
+        const unsigned long long key = (static_cast<unsigned long long>(delay_key(d1)) << 32) | br1;
+        if (key < best) {
+            best = key;
+            bestd = d1;
+        }
+    }
+    if (inf_classes && static_cast<uint32_t>(best >> 32) >= delay_key(__uint_as_float(0x7f800000u))) return false;
+    return true;
+}
+
+// One step of a run: pending broadcast receivers, the per-step rate table,
+// the race, the clock advance and the winner's transition, the time update.
+// CLASSES: the network's descriptors carry race classes (C <= 256).
+template <bool VERIFY, bool SLOTS, bool LOC8, bool CLASSES = false>
+static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32_t V, uint32_t P, uint32_t n_clocks,
+                                                bool rate_table, const RunView<LOC8> &rv, RunScalars &sc,
+                                                uint64_t seed, int var_id, uint64_t run, uint32_t &step,
+                                                float &time) {
+    const uint32_t bits = ceil_log2(C);
+    run_receivers<VERIFY, SLOTS, LOC8>(n, C, V, rv, sc, seed, var_id, run, step);
+
+    // ---- distinct rate programs, once per step
+    if (rate_table)
+        for (uint32_t j = 0; j < P; ++j) rv.rates[j] = inv_rate(eval(n, rv.vars, n.rate_prog[j]));
+
+    // ---- delays and the race
+    unsigned long long best;
+    float bestd;
+    if (CLASSES) {
+        if (!race_classes<LOC8>(n, C, bits, rv, seed, run, step, best, bestd))
+            race_exact<LOC8>(n, C, bits, rv, seed, run, step, best, bestd);
+    } else {
+        race_exact<LOC8>(n, C, bits, rv, seed, run, step, best, bestd);
     }
     const uint32_t win = bitrev_bits(static_cast<uint32_t>(best & 0xffffffffull), bits);
     run_commit<VERIFY, SLOTS, LOC8>(n, n_clocks, rv, sc, seed, var_id, run, step, time, win, bestd);

@@ -11,7 +11,8 @@
 // Template options: SLOTS keeps the slot masks; LOC8 stores locations as
 // 8-bit local indices (automata of at most 256 locations), otherwise as
 // 16-bit global indices; GSTATE puts the state in per-CTA global slabs when
-// it does not fit in shared memory.  The network layout comes from the
+// it does not fit in shared memory; CLASSES decides the race from race
+// classes (sim_run.cuh: race_classes).  The network layout comes from the
 // kernel parameters, so pointers into the staged network are rebuilt from
 // constants instead of occupying registers.
 //
@@ -26,7 +27,7 @@ namespace detail {
 #define CSMC_SERIAL_MIN_CTAS_PER_SM 5
 #endif
 
-template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE, bool CLASSES>
 __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kernel(const SimParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     stage_network(smem, p.blob, p.blob_bytes);
@@ -89,8 +90,8 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             continue;
         }
 
-        run_step<VERIFY, SLOTS, LOC8>(n, C, V, P, p.net.n_clocks, rate_table, rv, sc, p.seed, p.var_id, run, step,
-                                      time);
+        run_step<VERIFY, SLOTS, LOC8, CLASSES>(n, C, V, P, p.net.n_clocks, rate_table, rv, sc, p.seed, p.var_id, run,
+                                               step, time);
     }
     // lanes leave the loop at different times; aggregate per lane
     if (acc_hits) atomicAdd(p.scratch + 1, acc_hits);
@@ -100,18 +101,18 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
 
 }  // namespace detail
 
-template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE, bool CLASSES>
 int serial_launch_one(const SimParams &p, int grid, int block, size_t smem, void *stream) {
-    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE>;
+    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE, CLASSES>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     fn<<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return static_cast<int>(cudaGetLastError());
 }
 
-template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE>
+template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE, bool CLASSES>
 int serial_occupancy_one(int block, size_t smem, int *ctas) {
-    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE>;
+    auto fn = detail::serial_kernel<VERIFY, SLOTS, LOC8, GSTATE, CLASSES>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     return static_cast<int>(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, smem));

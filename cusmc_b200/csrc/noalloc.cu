@@ -139,6 +139,7 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         // memory when it fits, otherwise in slabs of the scratch array
         const bool slots = h.max_edges_per_loc >= 2;
         const bool loc8 = h.max_locs_per_comp <= 256;
+        const bool classes = (h.flags & CSMC_NET_RACE_CLASSES) != 0 && h.n_comps <= 256;
         const uint32_t blob_bytes = h.total_bytes;
         if (blob_bytes > static_cast<uint32_t>(max_smem))
             return fail(CSMC_ERR_LIMIT, "network does not fit in shared memory");
@@ -148,7 +149,7 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         const bool in_smem = blob_bytes + slab <= static_cast<size_t>(max_smem);
         const size_t smem = in_smem ? blob_bytes + slab : blob_bytes;
         int ctas = 0;
-        rc = csmc::serial_max_active_ctas(false, slots, loc8, !in_smem, block, smem, &ctas);
+        rc = csmc::serial_max_active_ctas(false, slots, loc8, !in_smem, classes, block, smem, &ctas);
         if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
         if (ctas < 1) return fail(CSMC_ERR_LIMIT, "kernel cannot be resident with this network");
         uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(ctas);
@@ -186,7 +187,7 @@ extern "C" int csmc_run_noalloc(const void *blob_host, const void *blob_device, 
         p.steps = steps;
         p.scratch = reinterpret_cast<unsigned long long *>(base);
         p.state_global = in_smem ? nullptr : base + kSlabOffset;
-        rc = csmc::serial_launch(false, slots, loc8, !in_smem, p, static_cast<int>(grid), block, smem, st);
+        rc = csmc::serial_launch(false, slots, loc8, !in_smem, classes, p, static_cast<int>(grid), block, smem, st);
         if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
         double *partials = reinterpret_cast<double *>(base + kPartialOffset);
         const bool need_values = q->kind == CSMC_QUERY_VARIABLE;
