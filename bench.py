@@ -389,17 +389,25 @@ def run_batch(args):
     ws = netgen.batch_networks()
     nets = [api.Network(_blob_of(w)) for w in ws]
     jobs = []
-    scale = BATCH_BUDGET_DIVISOR
+    scale = args.batch_divisor or BATCH_BUDGET_DIVISOR
     for i, (w, net) in enumerate(zip(ws, nets)):
         q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=1_000_000)
         jobs.append((net, q, SEED + i, max(10, w.runs // scale), rank * 10 ** 9))
     total = sum(j[3] for j in jobs)
+    t_start = time.perf_counter()
+
+    def progress(what):
+        print(f"[batch_64] {time.perf_counter() - t_start:8.1f} s  {what}", file=sys.stderr, flush=True)
+
+    progress(f"{len(jobs)} jobs, {total} runs")
     batch = api.Batch(jobs)
     t_tune = time.perf_counter()
     geometry = batch.autotune(probe_fraction=0.02)
     t_tune = time.perf_counter() - t_tune
+    progress(f"autotuned {geometry}")
     for _ in range(args.warmup):
-        batch.run(use_graph=True)
+        r0 = batch.run(use_graph=True)
+        progress(f"warm-up batch {r0[0].kernel_ms:.1f} ms")
     sampler = ClockSampler(local)
     sampler.start()
     batch_ms = []
@@ -418,6 +426,7 @@ def run_batch(args):
             t += r.kernel_ms
             seq_res.append(r)
         seq_ms.append(t)
+        progress(f"sequential pass {t:.1f} ms")
     same = all(a.hits == b.hits and a.steps == b.steps for a, b in zip(res, seq_res))
     value = total * args.steps / (sum(batch_ms) / 1000.0)
     seq_value = total * len(seq_ms) / (sum(seq_ms) / 1000.0)
@@ -451,10 +460,11 @@ def run_rare_is(args):
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
     t0 = time.perf_counter()
-    prop, log = P.train(net, q, seed=1, rounds=10, runs_per_round=100_000, adam_steps=30, lr=5e-3)
+    prop, log = P.train(net, q, seed=1, rounds=10, runs_per_round=100_000, adam_steps=10, lr=1e-2,
+                        max_rows=10_000_000)
     train_s = time.perf_counter() - t0
     # importance sampling until the 95% CI half-width is 10% of the estimate
-    chunk = 1_000_000
+    chunk = 100_000
     s1 = s2 = 0.0
     n = 0
     t1 = time.perf_counter()
@@ -510,6 +520,8 @@ def main():
     ap.add_argument("--runs", type=int, default=0,
                     help="runs per step per GPU (default: the workload's run count, 1e6 for the epidemic; "
                          "smaller values are for profiling captures)")
+    ap.add_argument("--batch-divisor", type=int, default=0,
+                    help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
     ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is"],
                     help="network and query (default: the 100-agent epidemic)")
     args = ap.parse_args()

@@ -93,6 +93,10 @@ _SIGNATURES = {
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),
     "csmc_smc": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
+    "csmc_smc_ex": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Query), ctypes.c_char_p,
+                                   ctypes.c_char_p, ctypes.c_char_p]),
+    "csmc_query_parse": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Query), ctypes.c_char_p,
+                                        ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]),
     "csmc_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                  ctypes.POINTER(ctypes.c_int32)]),
     "csmc_set_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -266,12 +266,29 @@ def smc(conf: Configuration, stat_conf: StatisticsConfiguration) -> None:
                          stat_conf.loc_query.encode()))
 
 
+def parse_query(xml_path: str, formula: str):
+    """An UPPAAL formula (Pr[<=T](<> P.loc), Pr[<=T](<> v >= k), E[<=T; N](max: v))
+    -> (Query, location name or "", run count or 0)."""
+    q = Query()
+    loc = ctypes.create_string_buffer(512)
+    sims = ctypes.c_uint64()
+    check(lib().csmc_query_parse(xml_path.encode(), formula.encode(), ctypes.byref(q), loc, 512, ctypes.byref(sims)))
+    return q, loc.value.decode(), sims.value
+
+
+def smc_ex(model: str, seed: int, sims: int, query: Query, loc_query: str = "", json_path: str | None = None,
+           runs_path: str | None = None) -> None:
+    """smc() with a full query and optional JSON summary / per-run CSV."""
+    check(lib().csmc_smc_ex(model.encode(), int(seed), int(sims), ctypes.byref(query), loc_query.encode(),
+                            json_path.encode() if json_path else None, runs_path.encode() if runs_path else None))
+
+
 def version() -> str:
     return lib().csmc_version().decode()
 
 
 __all__ = [
     "Batch", "Configuration", "StatisticsConfiguration", "Network", "Query", "Result", "compile_model", "dump_model",
-    "blob_info", "make_query", "location_query", "variable_query", "run_host", "smc", "version",
+    "blob_info", "make_query", "parse_query", "smc_ex", "location_query", "variable_query", "run_host", "smc", "version",
     "QUERY_LOCATION", "QUERY_VARIABLE", "_native",
 ]

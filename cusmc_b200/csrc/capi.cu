@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <cmath>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -556,11 +557,25 @@ int csmc_run_host(const void *blob, size_t bytes, const csmc_query *q, uint64_t 
     return rc;
 }
 
-int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int threshold, int var_id, int is_max,
-             int is_estimate, const char *loc_query) {
+}  // extern "C"
+
+namespace {
+
+std::string json_escape(const std::string &s) {
+    std::string o;
+    for (char c : s) {
+        if (c == '"' || c == '\\') o += '\\';
+        o += c;
+    }
+    return o;
+}
+
+// The reference's smc() flow (smc.cu:283-491) for one query, plus the
+// optional JSON summary and per-run dump of csmc_smc_ex.
+int smc_impl(const char *model_path, int seed, int sims, const csmc_query &q0, const std::string &lq,
+             const char *json_path, const char *runs_path) {
     if (!model_path) return fail(CSMC_ERR_ARG, "null model path");
-    const std::string lq = loc_query ? loc_query : "";
-    const bool loc_mode = var_id == -1;
+    const bool loc_mode = q0.kind == CSMC_QUERY_LOCATION;
     void *blob = nullptr;
     size_t bytes = 0;
     int rc = csmc_model_compile(model_path, lq.c_str(), loc_mode ? 1 : 0, &blob, &bytes);
@@ -569,6 +584,7 @@ int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int thr
     std::printf("Set number of variables to: %d\n", static_cast<int>(h->n_vars));
     std::fflush(stdout);
     const int mc = static_cast<int>(h->n_comps);
+    const double time_bound = q0.horizon;
     std::cout << "=================\n\n";
     std::cout << "Running SMC with the following settings:" << std::endl;
     std::cout << "- Number of simulations: " << sims << std::endl;
@@ -577,18 +593,13 @@ int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int thr
     std::cout << "- Time bound: " << time_bound << std::endl;
     std::cout << "- Num components: " << mc << std::endl;
     if (!loc_mode)
-        std::cout << "- Logging type: variable query. Finding " << (is_max ? "max" : "min")
-                  << " of variable with ID " << var_id << std::endl;
+        std::cout << "- Logging type: variable query. Finding " << (q0.is_max ? "max" : "min")
+                  << " of variable with ID " << q0.var_id << std::endl;
     else
         std::cout << "- Logging type: location query on query: " << lq << std::endl;
     std::cout << "=================\n\n";
 
-    csmc_query q{};
-    q.kind = loc_mode ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
-    q.var_id = var_id;
-    q.is_max = is_max;
-    q.is_estimate = is_estimate;
-    q.threshold = threshold;
+    csmc_query q = q0;
     q.horizon = static_cast<double>(static_cast<float>(time_bound));
     const uint64_t n_runs = sims > 0 ? static_cast<uint64_t>(sims) : 0;
     std::vector<uint8_t> flags(n_runs);
@@ -608,29 +619,118 @@ int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int thr
     std::cout << "Time taken: " << dur.count() << " on file " << model_path << std::endl;
     std::cout << "Time taken: " << dur.count() << " ns (" << (dur.count() / 1000000.0) << " ms)" << std::endl;
     write_timing_csv(model_path, mc, sims, time_bound, ms);
+    double result = 0, sum_sq = 0;
+    uint64_t hits = 0;
     if (!loc_mode) {
-        double result = 0;
-        if (is_estimate) {
-            for (uint64_t i = 0; i < n_runs; ++i) result += values[i];
+        if (q.is_estimate) {
+            for (uint64_t i = 0; i < n_runs; ++i) {
+                result += values[i];
+                sum_sq += values[i] * values[i];
+            }
             result = result / static_cast<double>(sims);
         } else {
             for (uint64_t i = 0; i < n_runs; ++i) {
-                if (is_max && values[i] > threshold) result += 1;
-                if (!is_max && values[i] < threshold) result += 1;
+                if (q.is_max && values[i] > q.threshold) ++hits;
+                if (!q.is_max && values[i] < q.threshold) ++hits;
             }
-            result = result / static_cast<double>(sims);
+            result = static_cast<double>(hits) / static_cast<double>(sims);
         }
         std::cout << "Result: " << result << std::endl;
     } else {
-        int hits = 0;
         for (uint64_t i = 0; i < n_runs; ++i)
             if (flags[i]) ++hits;
         std::cout << "Number of simulations: " << n_runs << std::endl;
         std::cout << "Number of hits: " << hits << std::endl;
         std::cout << "The answer to " << lq << " is "
                   << static_cast<float>(hits) / static_cast<float>(sims) << std::endl;
+        result = static_cast<double>(hits) / static_cast<double>(sims);
+    }
+    if (runs_path && *runs_path) {
+        std::ofstream o(runs_path);
+        if (!o) return fail(CSMC_ERR_ARG, std::string("cannot write ") + runs_path);
+        o << "run,flag,value\n";
+        o << std::setprecision(17);
+        for (uint64_t i = 0; i < n_runs; ++i) o << i << ',' << static_cast<int>(flags[i]) << ',' << values[i] << '\n';
+    }
+    if (json_path && *json_path) {
+        const double n = static_cast<double>(n_runs);
+        const bool estimate = !loc_mode && q.is_estimate;
+        double half = 0.0;
+        if (n_runs > 0) {
+            if (estimate) {
+                const double var = n > 1 ? std::max(0.0, (sum_sq - n * result * result) / (n - 1)) : 0.0;
+                half = 1.96 * std::sqrt(var / n);
+            } else {
+                half = 1.96 * std::sqrt(std::max(0.0, result * (1 - result)) / n);
+            }
+        }
+        const double delta = 0.05;
+        const double eps = n_runs ? std::sqrt(std::log(2 / delta) / (2 * n)) : 0.0;
+        std::ofstream o(json_path);
+        if (!o) return fail(CSMC_ERR_ARG, std::string("cannot write ") + json_path);
+        o << std::setprecision(17);
+        o << "{\"model\": \"" << json_escape(model_path) << "\", \"seed\": " << seed << ", \"simulations\": " << n_runs
+          << ", \"query\": {\"kind\": \"" << (loc_mode ? "location" : "variable") << "\", \"var_id\": " << q.var_id
+          << ", \"is_max\": " << q.is_max << ", \"is_estimate\": " << q.is_estimate << ", \"threshold\": " << q.threshold
+          << ", \"time_bound\": " << time_bound << ", \"location\": \"" << json_escape(lq) << "\"}"
+          << ", \"result\": " << result << ", \"hits\": " << hits << ", \"ci95\": [" << result - half << ", "
+          << result + half << "]"
+          << ", \"chernoff_hoeffding\": {\"delta\": " << delta << ", \"epsilon\": " << eps
+          << ", \"runs_for_epsilon_0_01\": " << std::ceil(std::log(2 / delta) / (2 * 0.01 * 0.01)) << "}"
+          << ", \"race_steps\": " << res.steps << ", \"capped_runs\": " << res.capped << ", \"ms\": " << ms << "}\n";
     }
     return CSMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int threshold, int var_id, int is_max,
+             int is_estimate, const char *loc_query) {
+    csmc_query q{};
+    q.kind = var_id == -1 ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
+    q.var_id = var_id;
+    q.is_max = is_max;
+    q.is_estimate = is_estimate;
+    q.threshold = threshold;
+    q.horizon = time_bound;
+    return smc_impl(model_path, seed, sims, q, loc_query ? loc_query : "", nullptr, nullptr);
+}
+
+int csmc_smc_ex(const char *model_path, int seed, int sims, const csmc_query *q, const char *loc_query,
+                const char *json_path, const char *runs_path) {
+    if (!q) return fail(CSMC_ERR_ARG, "null query");
+    return smc_impl(model_path, seed, sims, *q, loc_query ? loc_query : "", json_path, runs_path);
+}
+
+int csmc_query_parse(const char *xml_path, const char *formula, csmc_query *q, char *loc_query, size_t loc_cap,
+                     uint64_t *sims) {
+    if (!xml_path || !formula || !q) return fail(CSMC_ERR_ARG, "null argument");
+    std::unique_ptr<csmc::Network> net;
+    try {
+        net = csmc::parse_uppaal_file(xml_path);
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_MODEL, e.what());
+    }
+    try {
+        const csmc::QueryText t = csmc::parse_formula(*net, formula);
+        std::memset(q, 0, sizeof *q);
+        q->kind = t.kind == 0 ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
+        q->var_id = t.var_id;
+        q->is_max = t.is_max;
+        q->is_estimate = t.is_estimate;
+        q->threshold = t.threshold;
+        q->horizon = t.horizon;
+        if (loc_query) {
+            if (t.loc_query.size() + 1 > loc_cap) return fail(CSMC_ERR_ARG, "location buffer too small");
+            std::memcpy(loc_query, t.loc_query.c_str(), t.loc_query.size() + 1);
+        }
+        if (sims) *sims = t.sims;
+        return CSMC_OK;
+    } catch (const std::exception &e) {
+        return fail(CSMC_ERR_ARG, e.what());
+    }
 }
 
 }  // extern "C"

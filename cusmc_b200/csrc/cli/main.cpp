@@ -7,7 +7,12 @@
 //   -h|--help
 // Exit code 1 after a simulation, 0 after -h or a command-line error.
 // Options of this build that the reference does not have use the --csmc-
-// prefix so the reference grammar stays intact.
+// prefix so the reference grammar stays intact:
+//   --csmc-formula TEXT    the query as an UPPAAL formula (Pr[<=T](<> P.loc),
+//                          Pr[<=T](<> v >= k), E[<=T; N](max: v)); replaces the
+//                          -q fields except SIMS, which the formula's N overrides
+//   --csmc-json PATH       JSON summary (estimate, 95% CI, Chernoff-Hoeffding eps)
+//   --csmc-runs-csv PATH   every run's flag and tracked value
 #include "../../../include/csmc.h"
 
 #include <iostream>
@@ -15,6 +20,10 @@
 #include <string>
 
 namespace {
+
+struct Extras {  // the --csmc- options
+    std::string formula, json, runs_csv;
+};
 
 struct StatConfig {  // statistics_Configuration, main.cuh:46-58
     int simulations = 16384;
@@ -26,10 +35,17 @@ struct StatConfig {  // statistics_Configuration, main.cuh:46-58
     std::string loc_query;
 };
 
-bool handle_args(int argc, char **argv, std::string *filename, int *seed, StatConfig *stats) {
+bool handle_args(int argc, char **argv, std::string *filename, int *seed, StatConfig *stats, Extras *ex) {
     for (int i = 1; i < argc; i++) {
         std::string arg = argv[i];
-        if (arg == "-m" || arg == "--model") {
+        if (arg == "--csmc-formula" || arg == "--csmc-json" || arg == "--csmc-runs-csv") {
+            if (i + 1 >= argc) {
+                std::cerr << "Error: " << arg << " requires a value" << std::endl;
+                return false;
+            }
+            std::string &dst = arg == "--csmc-formula" ? ex->formula : (arg == "--csmc-json" ? ex->json : ex->runs_csv);
+            dst = argv[++i];
+        } else if (arg == "-m" || arg == "--model") {
             if (i + 1 < argc) {
                 *filename = argv[++i];
             } else {
@@ -99,9 +115,37 @@ int main(int argc, char *argv[]) {
     std::string filename = "../xml_files/LargeModels/aloha_50.xml";
     int seed = 1235;
     StatConfig st;
-    if (!handle_args(argc, argv, &filename, &seed, &st)) return 0;
-    const int rc = csmc_smc(filename.c_str(), seed, st.simulations, st.time_bound, st.threshold, st.var_id,
-                            st.is_max ? 1 : 0, st.is_estimate ? 1 : 0, st.loc_query.c_str());
+    Extras ex;
+    if (!handle_args(argc, argv, &filename, &seed, &st, &ex)) return 0;
+    int rc;
+    if (ex.formula.empty() && ex.json.empty() && ex.runs_csv.empty()) {
+        rc = csmc_smc(filename.c_str(), seed, st.simulations, st.time_bound, st.threshold, st.var_id,
+                      st.is_max ? 1 : 0, st.is_estimate ? 1 : 0, st.loc_query.c_str());
+    } else {
+        csmc_query q{};
+        std::string loc = st.loc_query;
+        int sims = st.simulations;
+        if (!ex.formula.empty()) {
+            char buf[512];
+            uint64_t n = 0;
+            rc = csmc_query_parse(filename.c_str(), ex.formula.c_str(), &q, buf, sizeof buf, &n);
+            if (rc != CSMC_OK) {
+                std::cerr << "Error: " << csmc_last_error() << std::endl;
+                return 0;
+            }
+            loc = buf;
+            if (n) sims = static_cast<int>(n);
+        } else {
+            q.kind = st.var_id == -1 ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
+            q.var_id = st.var_id;
+            q.is_max = st.is_max ? 1 : 0;
+            q.is_estimate = st.is_estimate ? 1 : 0;
+            q.threshold = st.threshold;
+            q.horizon = st.time_bound;
+        }
+        rc = csmc_smc_ex(filename.c_str(), seed, sims, &q, loc.c_str(), ex.json.empty() ? nullptr : ex.json.c_str(),
+                         ex.runs_csv.empty() ? nullptr : ex.runs_csv.c_str());
+    }
     if (rc != CSMC_OK) std::cerr << "Error: " << csmc_last_error() << std::endl;
     return 1;
 }

@@ -88,10 +88,12 @@ struct Network {
     std::vector<Node> nodes;                           // document order
     std::unordered_map<int, std::vector<Edge>> edges;  // source node id -> edges, document order
     std::vector<VarDecl> vars;                         // id order
+    std::vector<std::string> var_names;                // id order: "name" (global), "Template.name" (local)
     std::vector<int> start_nodes;                      // init node id per template (document order)
     std::unordered_map<int, std::string> node_names;   // only named locations
     std::vector<std::pair<int, std::string>> node_name_order;  // insertion order of node_names
     std::unordered_map<int, std::string> template_names;
+    std::string system_text;  // the <system> block (process instantiations)
     int n_templates = 0;
     Expr *make(Op op) {
         arena.emplace_back();
@@ -178,5 +180,16 @@ std::vector<uint8_t> pack_device_model(const DevModel &m);
 
 // Helpers shared with the CLI.
 std::string quote_dump(const std::string &s);
+
+// A query formula of the reference's model files, resolved against a network
+// (front/query.cpp).  kind: 0 location, 1 variable; sims: the formula's run
+// count (0: none given).
+struct QueryText {
+    int kind = 0, var_id = -1, is_max = 1, is_estimate = 0;
+    double threshold = 0.0, horizon = 0.0;
+    uint64_t sims = 0;
+    std::string loc_query;
+};
+QueryText parse_formula(const Network &net, const std::string &formula);
 
 }  // namespace csmc

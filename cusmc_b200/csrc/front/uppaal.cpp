@@ -569,10 +569,12 @@ class UppaalReader {
         const XmlNode *nta = doc.child("nta");
         if (!nta) fail("model has no <nta> element");
         init_globals(*nta);
+        net_.system_text = nta->child_text("system");
         int system = 0;
         for (const XmlNode *t : nta->children_named("template")) {
             const std::string init_ref = remove_spaces(t->child(("init")) ? t->child("init")->attr("ref") : "");
             init_node_id_ = node_id(init_ref);
+            cur_template_ = t->child_text("name");
             init_locals(*t);
             net_.template_names.emplace(system, t->child_text("name"));
             for (const XmlNode *l : t->children_named("location")) location(*l, system);
@@ -589,6 +591,7 @@ class UppaalReader {
     Network &net_;
     DeclParser dp_;
     int vars_id_ = 0, chan_id_ = 1, init_node_id_ = 0;
+    std::string cur_template_;
     std::unordered_map<std::string, double> const_local_, const_global_;
     std::unordered_map<std::string, int> timers_, global_timers_, vars_, global_vars_;
 
@@ -615,6 +618,7 @@ class UppaalReader {
         (global ? global_vars_ : vars_)[name] = vars_id_;
         if (clock) (global ? global_timers_ : timers_)[name] = vars_id_;
         net_.vars.push_back(VarDecl{vars_id_, clock ? 1 : 0, value});
+        net_.var_names.push_back(global ? name : remove_spaces(cur_template_) + "." + name);
         ++vars_id_;
     }
 

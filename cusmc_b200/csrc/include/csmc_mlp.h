@@ -106,6 +106,16 @@ CSMC_HD float gelu_grad_f(float x) {
     return f_fma(f_mul(x, ds), dz, s);
 }
 
+/* GELU and its derivative sharing one sigmoid (the same bits as gelu_f and
+ * gelu_grad_f). */
+CSMC_HD void gelu_both(float x, float &g, float &dg) {
+    const float s = sigmoid_f(gelu_arg(x));
+    const float ds = f_mul(s, f_add(1.0f, -s));
+    const float dz = f_mul(1.59576912f, f_fma(f_mul(0.134145f, x), x, 1.0f));
+    g = f_mul(x, s);
+    dg = f_fma(f_mul(x, ds), dz, s);
+}
+
 /* Features of location class l (local index modulo 4) given the run's
  * variables v[0..3] (n_int of them present), components C, time t and
  * horizon T; BF16-rounded. */

@@ -32,9 +32,9 @@ constexpr uint32_t kTmemCols = 256;             // D1/D3 [0,64), D2 [64,128), D4
 constexpr uint32_t kColD1 = 0, kColD2 = 64, kColD4 = 128;
 constexpr int kN4 = 96;                         // [H1 (64) | X (16) | 1 | 0 x 15]
 
-// shared-memory carve-up (bytes); the slack at the end keeps every operand
-// access inside the allocation even under a transposed reading of the
-// descriptor strides
+// shared-memory carve-up (bytes); every operand tile ends before kGz1, and
+// the allocation extends 66 KB beyond it, so operand accesses stay inside
+// the allocation even under a transposed reading of the descriptor strides
 constexpr uint32_t kA1 = 0;                     // X tile      128 x 16
 constexpr uint32_t kB1 = kA1 + 128 * 16 * 2;    // W1          64 x 16
 constexpr uint32_t kA2 = kB1 + 64 * 16 * 2;     // H1 tile     128 x 64
@@ -44,9 +44,10 @@ constexpr uint32_t kB3 = kA3 + 128 * 64 * 2;    // W2^T        64 x 64 (in x out
 constexpr uint32_t kA4 = kB3 + 64 * 64 * 2;     // dZ^T        128 x 128 (neuron x row)
 constexpr uint32_t kB4 = kA4 + 128 * 128 * 2;   // F^T         96 x 128 (feature x row)
 constexpr uint32_t kGz1 = kB4 + kN4 * 128 * 2;  // GELU'(z1) per thread, interleaved: 64 x 128 floats
-constexpr uint32_t kMisc = kGz1 + 64 * 128 * 4;  // mbarrier, tmem address, biases, reductions
+constexpr uint32_t kGz2 = kGz1 + 64 * 128 * 4;  // GELU'(z2) per thread, interleaved: 64 x 128 floats
+constexpr uint32_t kMisc = kGz2 + 64 * 128 * 4;  // mbarrier, tmem address, biases, reductions
 constexpr uint32_t kMiscBytes = 2048;
-constexpr uint32_t kSmemBytes = kMisc + kMiscBytes + 16 * 1024;
+constexpr uint32_t kSmemBytes = kMisc + kMiscBytes;
 
 constexpr uint32_t kWaitLimit = 1u << 20;       // bounded mbarrier polls
 
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(128, 1)
     float *b2s = reinterpret_cast<float *>(sm + kMisc + 768);
     float *w3s = reinterpret_cast<float *>(sm + kMisc + 1024);
     float *gz1 = reinterpret_cast<float *>(sm + kGz1);          // [64][128]
+    float *gz2 = reinterpret_cast<float *>(sm + kGz2);          // [64][128]
     const uint32_t mbar_a = smem_u32(mbar);
 
     // ---- constant operands: W1 (B1), W2 (B2), W2^T (B3), the ones column of B4
@@ -222,8 +224,10 @@ __global__ void __launch_bounds__(128, 1)
                 for (int i = 0; i < 16; ++i) {
                     const int j = 16 * c + i;
                     const float zz = f_add(z[i], b1s[j]);
-                    const float h = bf16_round(gelu_f(zz));
-                    if (MODE == 1) gz1[j * 128 + tid] = gelu_grad_f(zz);
+                    float gv, dg;
+                    gelu_both(zz, gv, dg);
+                    const float h = bf16_round(gv);
+                    if (MODE == 1) gz1[j * 128 + tid] = dg;
                     st_bf16(sm + kA2, kmaj(tid, j, kRows), h);
                     if (MODE == 1) st_bf16(sm + kB4, kmaj(j, tid, kN4), h);
                 }
@@ -247,9 +251,12 @@ __global__ void __launch_bounds__(128, 1)
         for (int c = 0; c < 4; ++c) tmem_ld16(tmem + lane_base + kColD2 + 16 * c, z2 + 16 * c);
         float th = b3;
 #pragma unroll
-        for (int k = 0; k < 64; ++k) {
-            z2[k] = f_add(z2[k], b2s[k]);
-            th = f_fma(gelu_f(z2[k]), w3s[k], th);
+        for (int k = 0; k < 64; ++k) {  // z2[k] becomes GELU(z2 + b2); the derivative goes to gz2
+            float gv, dg;
+            gelu_both(f_add(z2[k], b2s[k]), gv, dg);
+            z2[k] = gv;
+            if (MODE == 1) gz2[k * 128 + tid] = dg;
+            th = f_fma(gv, w3s[k], th);
         }
         const bool inside = th >= -CSMC_MLP_THETA_MAX && th <= CSMC_MLP_THETA_MAX;
         const float thc = inside ? th : (th < 0.0f ? -CSMC_MLP_THETA_MAX : CSMC_MLP_THETA_MAX);
@@ -269,11 +276,11 @@ __global__ void __launch_bounds__(128, 1)
         if (lane == 0) atomicAdd(&red[64], gs);
 #pragma unroll
         for (int k = 0; k < 64; ++k) {
-            float v = f_mul(g, gelu_f(z2[k]));
+            float v = f_mul(g, z2[k]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) atomicAdd(&red[k], v);
-            const float dz = f_mul(f_mul(g, w3s[k]), gelu_grad_f(z2[k]));
+            const float dz = f_mul(f_mul(g, w3s[k]), gz2[k * 128 + tid]);
             st_bf16(sm + kA3, kmaj(tid, k, kRows), dz);
             st_bf16(sm + kA4, kmaj(k, tid, kRows), dz);
         }

@@ -261,22 +261,19 @@ static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, ui
                 const uint32_t br = bitrev_bits(cc, bits);
                 const uint32_t g = CSMC_DESC_CLASS(fl);
                 if (g < CSMC_RACE_CLASSES) {
+                    // branch-free update of the class's two largest keys
+                    // (slots of absent classes hold stale values; the
+                    // presence bits decide)
                     const uint32_t key = (x & 0xffffff00u) | (255u - br);
                     const uint32_t bit = 1u << g;
                     uint32_t *k1 = rv.cls + g * T, *k2 = rv.cls + (CSMC_RACE_CLASSES + g) * T;
-                    if (!(pres & bit)) {
-                        *k1 = key;
-                        pres |= bit;
-                    } else {
-                        const uint32_t a = *k1;
-                        if (key > a) {
-                            *k1 = key;
-                            *k2 = a;
-                        } else if (!(pres2 & bit) || key > *k2) {
-                            *k2 = key;
-                        }
-                        pres2 |= bit;
-                    }
+                    const uint32_t a = *k1, b = *k2;
+                    const bool p1 = (pres & bit) != 0, p2 = (pres2 & bit) != 0;
+                    const bool gt1 = !p1 || key > a;
+                    *k1 = gt1 ? key : a;
+                    *k2 = gt1 ? (p1 ? a : b) : ((!p2 || key > b) ? key : b);
+                    pres2 |= pres & bit;
+                    pres |= bit;
                 } else {
                     float d;
                     if (fl & CSMC_DESC_ZERO) {

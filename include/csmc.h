@@ -131,6 +131,26 @@ int csmc_run_verify(const csmc_net *net, const csmc_query *q, uint64_t seed, uin
 int csmc_smc(const char *model_path, int seed, int sims, int time_bound, int threshold, int var_id, int is_max,
              int is_estimate, const char *loc_query);
 
+/* csmc_smc with a full query (double threshold and horizon) and, beyond the
+ * reference's report, optional outputs (no counterpart in the reference):
+ * json_path (may be NULL) receives a JSON summary with the estimate, its 95%
+ * confidence interval (normal approximation) and the Chernoff-Hoeffding
+ * epsilon at delta = 0.05; runs_path (may be NULL) a CSV of every run's
+ * flag and tracked value. */
+int csmc_smc_ex(const char *model_path, int seed, int sims, const csmc_query *q, const char *loc_query,
+                const char *json_path, const char *runs_path);
+
+/* Reads an UPPAAL query formula as the reference's model files write them
+ * (no counterpart in the reference, which takes the query from its command
+ * line): Pr[<=T](<> Template.location), Pr[<=T](<> var OP k) with OP one of
+ * >= > <= <, an optional run count Pr[<=T; N], and E[<=T; N](max: var) /
+ * E[<=T; N](min: var).  Variables are named as declared (template locals as
+ * Template.name).  Fills *q (max_steps 0), the location name for location
+ * queries (loc_query, capacity loc_cap; "" otherwise) and *sims (the
+ * formula's run count, 0 when absent). */
+int csmc_query_parse(const char *xml_path, const char *formula, csmc_query *q, char *loc_query, size_t loc_cap,
+                     uint64_t *sims);
+
 /* Sizes a launch would use for this network: lanes per run, components per
  * lane, runs per CTA. */
 int csmc_plan(const csmc_net *net, int32_t *lanes_per_run, int32_t *comps_per_lane, int32_t *runs_per_cta);

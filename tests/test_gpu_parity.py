@@ -179,3 +179,45 @@ def test_production_kernel_matches_verify_kernel():
     assert np.array_equal(values.cpu().numpy(), out["values"])
     assert np.array_equal(steps.cpu().numpy().view(np.uint32), out["steps"])
     assert r.hits == r2.hits and r.steps == r2.steps
+
+
+def _class_stress_network(kind):
+    """Networks whose race classes hit the exact-race fallback often.
+    ties: a class of 24 components with rate 3e38 (1/rate is a denormal
+    float, so most draws give equal delays) beside a class of rate-1
+    components; inf: components that move to a location whose rate program
+    evaluates to 0 (1/rate = +inf), until every delay is infinite."""
+    from cusmc_b200.netgen import Workload, _Doc
+    d = _Doc("int hits = 0;\nint zero = 0;\nint big = 1;")
+    if kind == "ties":
+        for c in range(24):
+            a = d.new_id()
+            d.template(f"F{c}", "", [(a, "a", [("exponentialrate", "big * 3000000000000000000.0 * 100000000000000000000.0")])],
+                       a, [(a, a, [("assignment", "hits = hits + 1")])])
+        for c in range(8):
+            a = d.new_id()
+            d.template(f"S{c}", "", [(a, "a", [("exponentialrate", "1")])], a, [(a, a, [("assignment", "hits = hits + 1")])])
+    else:
+        for c in range(8):
+            live, dead = d.new_id(), d.new_id()
+            d.template(f"D{c}", "", [(live, "live", [("exponentialrate", "1")]),
+                                     (dead, "dead", [("exponentialrate", "zero * 2.0")])],
+                       live, [(live, dead, [("assignment", "hits = hits + 1")])])
+    return Workload(f"class_{kind}", d.finish(), var_id=0, threshold=5, horizon=50, runs=256)
+
+
+@pytest.mark.parametrize("kind", ["ties", "inf"])
+def test_race_class_fallbacks(kind):
+    import struct
+    w = _class_stress_network(kind)
+    blob = _blob(w)
+    flags = struct.unpack_from("<I", blob, 112)[0]
+    info = api.blob_info(blob)
+    q = api.variable_query(0, w.horizon, threshold=w.threshold, is_max=True, max_steps=3000)
+    if kind == "ties":
+        # the rate program must evaluate to a finite float rate with a denormal reciprocal
+        import oracle
+        r, _, _ = oracle.run(blob, q, 1, 4, threads=1)
+        assert r.steps > 0
+    assert flags & 2, "the network should carry race classes"
+    _compare(blob, q, seed=99, n_runs=256)
