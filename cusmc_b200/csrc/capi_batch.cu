@@ -84,8 +84,9 @@ void drop_graph(csmc_batch *b) {
     b->exec = nullptr;
 }
 
-// Job table in run-space order for the given per-job run counts.
-std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<uint64_t> &runs) {
+// Job table in run-space order for the given per-job run counts; step_cap
+// (0: none) limits every run's race steps (autotuner probes).
+std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<uint64_t> &runs, uint64_t step_cap = 0) {
     std::vector<csmc::BatchJob> t(b->n_jobs);
     uint64_t begin = 0;
     for (int k = 0; k < b->n_jobs; ++k) {
@@ -101,6 +102,7 @@ std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<u
         J.first_run = b->first_runs[j];
         J.seed = b->seeds[j];
         J.max_steps = q.max_steps ? q.max_steps : 10000000ull;
+        if (step_cap && J.max_steps > step_cap) J.max_steps = step_cap;
         J.threshold = q.threshold;
         J.horizon = static_cast<float>(q.horizon);
         J.loc_mode = q.kind == CSMC_QUERY_LOCATION;
@@ -117,8 +119,8 @@ std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<u
     return t;
 }
 
-int upload_table(csmc_batch *b, const std::vector<uint64_t> &runs) {
-    const std::vector<csmc::BatchJob> t = build_table(b, runs);
+int upload_table(csmc_batch *b, const std::vector<uint64_t> &runs, uint64_t step_cap = 0) {
+    const std::vector<csmc::BatchJob> t = build_table(b, runs, step_cap);
     CK(cudaMemcpy(b->d_jobs, t.data(), t.size() * sizeof(csmc::BatchJob), cudaMemcpyHostToDevice),
        "cudaMemcpy(job table)");
     return CSMC_OK;
@@ -207,8 +209,12 @@ void fill_results(const csmc_batch *b, const std::vector<uint64_t> &runs, float 
 
 // Probe of the batch at the current geometry with the given run counts:
 // device time in ms; per-job steps in steps_out (job order).
+// Probes cap every run at kProbeSteps race steps, so that a probe costs a
+// bounded amount of work even when single runs of a job take seconds.
+constexpr uint64_t kProbeSteps = 2000;
+
 int probe(csmc_batch *b, const std::vector<uint64_t> &runs, float *ms, std::vector<uint64_t> *steps_out) {
-    int rc = upload_table(b, runs);
+    int rc = upload_table(b, runs, kProbeSteps);
     if (rc) return rc;
     const uint64_t total = std::accumulate(runs.begin(), runs.end(), uint64_t{0});
     cudaStream_t st = nullptr;
@@ -218,9 +224,10 @@ int probe(csmc_batch *b, const std::vector<uint64_t> &runs, float *ms, std::vect
     CK(cudaEventRecord(b->ev1, st), "cudaEventRecord");
     CK(cudaStreamSynchronize(st), "batch probe");
     CK(cudaEventElapsedTime(ms, b->ev0, b->ev1), "cudaEventElapsedTime");
-    if (steps_out) {
+    if (steps_out) {  // per job: steps, or 0 when some run hit the probe's cap
         steps_out->assign(b->n_jobs, 0);
-        for (int k = 0; k < b->n_jobs; ++k) (*steps_out)[b->order[k]] = b->h_counters[2 + 4 * k];
+        for (int k = 0; k < b->n_jobs; ++k)
+            (*steps_out)[b->order[k]] = b->h_counters[3 + 4 * k] ? 0 : b->h_counters[2 + 4 * k];
     }
     return CSMC_OK;
 }
@@ -409,8 +416,8 @@ int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_p
     float ms = 0.0f;
     int rc = probe(b, runs, &ms, &steps);
     if (rc) return rc;
-    for (int j = 0; j < b->n_jobs; ++j)
-        if (runs[j])
+    for (int j = 0; j < b->n_jobs; ++j)  // measured cost per run where no probe run was capped
+        if (runs[j] && steps[j])
             b->cost[j] = static_cast<double>(steps[j]) / runs[j] * std::max<uint32_t>(1, b->nets[j]->h.n_comps);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->cost[x] > b->cost[y]; });
     // 2. geometry: threads per CTA x CTAs per SM

@@ -24,7 +24,7 @@ namespace csmc {
 namespace detail {
 
 #ifndef CSMC_SERIAL_MIN_CTAS_PER_SM
-#define CSMC_SERIAL_MIN_CTAS_PER_SM 5
+#define CSMC_SERIAL_MIN_CTAS_PER_SM 4
 #endif
 
 template <bool VERIFY, bool SLOTS, bool LOC8, bool GSTATE, bool CLASSES>

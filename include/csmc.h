@@ -221,10 +221,11 @@ int csmc_batch_outputs_host(const csmc_batch *b, int32_t job, uint8_t *flags, do
                             uint64_t *digests, uint32_t *final_state);
 
 /* Autotuner for the batch: runs a probe batch (each job's runs scaled by
- * probe_fraction, at least one run) at each candidate geometry (64 and 128
- * threads per CTA, every CTAs-per-SM count that fits), keeps the fastest, and
- * orders the jobs in the run space by measured cost per run, most expensive
- * first, so that the cheapest runs fill the end of the batch. */
+ * probe_fraction, at least one run, every run capped at 2000 race steps) at
+ * each candidate geometry (64 and 128 threads per CTA, every CTAs-per-SM
+ * count that fits), keeps the fastest, and orders the jobs in the run space
+ * by measured cost per run (where no probe run reached the cap), most
+ * expensive first, so that the cheapest runs fill the end of the batch. */
 int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_per_cta, int32_t *ctas_per_sm);
 
 void csmc_batch_free(csmc_batch *b);
