@@ -124,6 +124,7 @@ _SIGNATURES = {
     "csmc_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
     "csmc_batch_free": (None, [ctypes.c_void_p]),
+    "csmc_is_set_inference": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "csmc_is_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_char_p, ctypes.c_uint64,
                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),

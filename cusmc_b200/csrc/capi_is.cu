@@ -63,14 +63,15 @@ int plan_is(const csmc_net *n, bool trace, uint64_t n_runs, Launch &L) {
     L.slots = h.max_edges_per_loc >= 2;
     L.loc8 = h.max_locs_per_comp <= 256;
     const size_t per = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, L.loc8);
-    L.smem = n->bytes + csmc::is_mlp_smem_bytes() + ((per * L.block + 15) & ~static_cast<size_t>(15));
+    L.smem = n->bytes + csmc::is_mlp_smem_bytes() + (n->is_tc ? csmc::is_stage_bytes(L.block) : 0) +
+             ((per * L.block + 15) & ~static_cast<size_t>(15));
     int max_smem = 0, sms = 0, ctas = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device), "device attribute");
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device), "device attribute");
     if (L.smem > static_cast<size_t>(max_smem))
         return fail(CSMC_ERR_LIMIT, "importance sampling needs the network, the proposal network and the run state "
                                     "of 128 runs in shared memory (" + std::to_string(L.smem) + " bytes)");
-    int rc = csmc::is_max_active_ctas(trace, L.slots, L.loc8, L.block, L.smem, &ctas);
+    int rc = csmc::is_max_active_ctas(n->is_tc, trace, L.slots, L.loc8, L.block, L.smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "importance-sampling kernel cannot be resident");
     uint64_t grid = static_cast<uint64_t>(sms) * ctas;
@@ -112,6 +113,12 @@ int check_query(const csmc_net *n, const csmc_query *q) {
 
 extern "C" {
 
+int csmc_is_set_inference(csmc_net *n, int32_t tensor_cores) {
+    if (!n) return fail(CSMC_ERR_ARG, "null argument");
+    n->is_tc = tensor_cores != 0;
+    return CSMC_OK;
+}
+
 int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t seed, uint64_t first_run,
                 uint64_t n_runs, uint8_t *flags, double *logw, double *values, uint32_t *steps, csmc_result *out,
                 void *stream) {
@@ -143,7 +150,7 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
     ip.logw = logw;
     ip.wvals = n->d_wvals;
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
-    rc = csmc::is_launch(false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
+    rc = csmc::is_launch(n->is_tc, false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "importance-sampling kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
     reduce_weights<<<csmc::kReduceBlocks, 256, 0, st>>>(n->d_wvals, n_runs, n->d_partials);
@@ -188,7 +195,7 @@ int csmc_is_trace(csmc_net *n, const csmc_query *q, const void *params, uint64_t
     ip.trace_w = weights;
     ip.row_offset = row_offset;
     ip.rows = static_cast<csmc::MlpRow *>(rows);
-    rc = csmc::is_launch(true, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
+    rc = csmc::is_launch(n->is_tc, true, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "replay kernel launch");
     CK(cudaStreamSynchronize(st), "replay kernel");
     return CSMC_OK;

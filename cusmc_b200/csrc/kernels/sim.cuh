@@ -150,10 +150,16 @@ struct IsParams {
     MlpRow *rows;                 // trace mode: the rows
 };
 
-int is_launch(bool trace, bool slots, bool loc8, const IsParams &p, int grid, int block, size_t smem, void *stream);
-int is_max_active_ctas(bool trace, bool slots, bool loc8, int block, size_t smem, int *ctas);
-// Shared memory of the importance-sampling kernel besides network and state.
+// tc: theta by warp-level tensor-core MMAs (else the CUDA-core evaluation
+// that is bit-identical to the CPU oracle).
+int is_launch(bool tc, bool trace, bool slots, bool loc8, const IsParams &p, int grid, int block, size_t smem,
+              void *stream);
+int is_max_active_ctas(bool tc, bool trace, bool slots, bool loc8, int block, size_t smem, int *ctas);
+// Shared memory of the importance-sampling kernels besides network and
+// state: the proposal network, and (tensor-core kernel) each warp's staging
+// area of 128 feature rows.
 size_t is_mlp_smem_bytes();
+__host__ __device__ inline size_t is_stage_bytes(uint32_t threads) { return static_cast<size_t>(threads / 32) * 128 * 8 * 4; }
 
 // Tensor-core kernels of the proposal network (mlp_train.cu): mode 0 writes
 // theta per row, mode 1 gradient partials per CTA (mlp_tc_partial_floats()

@@ -117,6 +117,12 @@ def _ptr(t) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+def set_inference(net, tensor_cores: bool) -> None:
+    """Tensor-core evaluation of the proposal (default) or the CUDA-core one
+    that reproduces the CPU oracle bit for bit."""
+    check(lib().csmc_is_set_inference(net._h, 1 if tensor_cores else 0))
+
+
 def is_run(net, query: Query, params: bytes, seed: int, n_runs: int, first_run: int = 0, flags=None, logw=None,
            values=None, steps=None, stream=None) -> Result:
     """csmc_is_run on a Network; per-run outputs are optional torch CUDA tensors."""

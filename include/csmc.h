@@ -237,6 +237,12 @@ void csmc_batch_free(csmc_batch *b);
  * csmc_mlp.h (CSMC_MLP_PARAM_BYTES bytes). */
 #define CSMC_MLP_PARAM_BYTES 11024
 
+/* How runs under the proposal evaluate theta (default 1): 1 = warp-level
+ * BF16 tensor-core MMAs with FP32 accumulation; 0 = CUDA cores in the CPU
+ * oracle's operation order (bit-identical runs).  Weights and estimates are
+ * exact for the theta a run used either way. */
+int csmc_is_set_inference(csmc_net *net, int32_t tensor_cores);
+
 /* Runs first_run .. first_run+n_runs-1 under the proposal.  Per-run device
  * outputs (may be NULL): flags, logw (log-likelihood ratio nominal/proposal,
  * FP64), values (tracked max/min), steps.  out->sum / sum_sq are the sums of
