@@ -196,8 +196,10 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev).cuda_stream
 
+    from cusmc_b200 import shard
+
     def first_run_of(step):
-        return (step * world + rank) * n
+        return shard.first_run(step, rank, world, n)
 
     for s in range(args.warmup):
         net.run(q, SEED, n, first_run_of(1000 + s), flags=flags, values=values, stream=stream)
@@ -226,13 +228,7 @@ def run_ours(args):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_total = sum(step_ms)
     t_kernel = sum(kernel_ms)
-    if world > 1:
-        t = torch.tensor([t_total, t_kernel], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total, t_kernel = t.tolist()
-        c = torch.tensor([hits, steps_total], dtype=torch.int64, device=dev)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        hits, steps_total = c.tolist()
+    (hits, steps_total), (t_total, t_kernel) = shard.combine([hits, steps_total], [t_total, t_kernel], dev)
     runs_total = n * args.steps * world
     value = runs_total / (t_total / 1000.0)
 
