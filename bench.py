@@ -2,11 +2,14 @@
 epidemic network, Pr[<=100](<> R >= 50), 1,000,000 runs per step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload epidemic_100|random_0|mutex_8|mutex_32|mutex_64|mutex_256]
+                  [--workload epidemic_100|random_0|mutex_8|mutex_32|mutex_64|mutex_256|batch_64|rare_is]
 
 The default workload is the epidemic; the others (the small random network
 and the Fischer-style mutex at n = 8, 32, 64, 256) use the same measurement
-with their own run counts (1e4 and 1e7 runs per step).
+with their own run counts (1e4 and 1e7 runs per step).  batch_64 times 64
+random networks in one graph-captured persistent launch against 64
+sequential launches; rare_is times learned importance sampling (CE training
+included) to a 10%-relative-error interval against plain SMC's rate.
 
 A step is one pass of the hot path over one batch: 1e6 independent runs of
 the epidemic network (seeded synthetic input: the network comes from
