@@ -35,8 +35,13 @@ def test_reference_report_and_timing_csv(tmp_path):
     res = float(re.search(r"^Result: (\S+)", p.stdout, re.M).group(1))
     assert 0.0 < res < 1.0
     assert re.search(r"^Time taken: \S+ ms on file ", p.stdout, re.M)
+    # write_csv.cu layout: header row with an empty corner cell, then one
+    # column per MC<components>_Sim<runs>_Time<T> configuration; one row per
+    # model file with the time in ms
     rows = list(csv.reader(open(tmp_path / "results5.csv"), delimiter=";"))
-    assert rows[0][0] != "" and any("epi.xml" in r[0] for r in rows[1:])
+    assert rows[0][0] == "" and rows[0][1] == "MC30_Sim4096_Time100.00"
+    row = next(r for r in rows[1:] if r[0] == "epi.xml")
+    assert float(row[1]) > 0.0
 
 
 def test_formula_json_and_run_dump_match_the_library(tmp_path):
