@@ -42,6 +42,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -509,6 +511,59 @@ def run_rare_is(args):
         print(json.dumps(line))
 
 
+def run_mlp_grad(args):
+    """The tcgen05 gradient kernel of the proposal network on a seeded
+    synthetic row set shaped like the epidemic's training rows (one-hot class,
+    S/E/I/R fractions, t/T; a, b weights): rows/s and tensor TFLOP/s.
+    FLOP per row counted as the MMAs issue them: forward 2*(16*64 + 64*64),
+    back-propagation 2*64*64, weight-gradient GEMM 2*128*96."""
+    import torch
+    from cusmc_b200 import proposal as P
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    n = args.runs or 4_000_000
+    rng = np.random.default_rng(SEED)
+    x = np.zeros((n, 16), np.float32)
+    x[np.arange(n), rng.integers(0, 4, n)] = 1.0
+    frac = rng.dirichlet([4, 1, 1, 4], n).astype(np.float32)
+    x[:, 5:9] = frac
+    x[:, 9] = rng.uniform(0, 1, n)
+    rows = np.zeros(n, dtype=np.dtype([("x", "<u2", (16,)), ("a", "<f4"), ("b", "<f4")]))
+    rows["x"] = P.f32_to_bf16_bits(x.ravel()).reshape(n, 16)
+    rows["a"] = rng.exponential(1e-3, n).astype(np.float32)
+    rows["b"] = (rng.uniform(0, 1, n) < 0.25).astype(np.float32) * 1e-3
+    d_rows = torch.from_numpy(rows.view(np.uint8).copy()).cuda()
+    prop = P.Proposal.init(1)
+    prop.w3 = (rng.standard_normal(64) * 0.05).astype(np.float32)
+    params = prop.pack()
+    for _ in range(args.warmup):
+        P.mlp_grad(params, d_rows, n)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(args.steps):
+        P.mlp_grad(params, d_rows, n)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    flop_row = 2 * (16 * 64 + 64 * 64) + 2 * 64 * 64 + 2 * 128 * 96
+    peak = 1672.1
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peak = json.load(open(pk)).get("bf16_tflops", peak)
+    tflops = flop_row * n / (ms / 1000.0) / 1e12
+    line = {"metric": "rows/s of the tensor-core CE gradient (proposal network)", "value": n / (ms / 1000.0),
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 operands / f32 accumulation", "data": "synthetic rows (seeded)",
+            "config": {"workload": f"mlp_grad, {n} rows", "flop_per_row": flop_row},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tflops / peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops"
+                         if os.path.exists(pk) else "fallback"},
+            "note": "time per call includes the parameter upload, partial-sum copy and allocation of the call"}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -521,14 +576,16 @@ def main():
                          "smaller values are for profiling captures)")
     ap.add_argument("--batch-divisor", type=int, default=0,
                     help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
-    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is"],
+    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "mlp_grad"],
                     help="network and query (default: the 100-agent epidemic)")
     args = ap.parse_args()
     if args.workload == "batch_64" and args.impl == "ours":
         return run_batch(args)
     if args.workload == "rare_is" and args.impl == "ours":
         return run_rare_is(args)
-    if args.workload in ("batch_64", "rare_is"):
+    if args.workload == "mlp_grad" and args.impl == "ours":
+        return run_mlp_grad(args)
+    if args.workload in ("batch_64", "rare_is", "mlp_grad"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference simulates one model per process and has "
                           "no importance sampling; this workload has no reference arm"}))
         return
