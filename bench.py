@@ -73,6 +73,10 @@ def _netgen():
 # the rare event of the importance-sampling workload: (T, threshold) with
 # goal R > threshold (plain-SMC probability about 1e-6)
 IS_RARE = (75, 94)
+# CE training of the rare_is workload: up to 12 rounds of 1e4 runs, 40 Adam
+# steps per round on at most 1e6 rows, stop once a round's level is the goal
+IS_CE = dict(rounds=12, runs_per_round=10_000, adam_steps=40, lr=3e-2, max_rows=1_000_000, settle=1)
+IS_CHUNK = 20_000
 # the batch workload's run budgets (log-uniform in [1e3, 1e6]) are divided by
 # this so that one batch takes seconds (the full budgets take minutes)
 BATCH_BUDGET_DIVISOR = 100
@@ -461,11 +465,10 @@ def run_rare_is(args):
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
     t0 = time.perf_counter()
-    prop, log = P.train(net, q, seed=1, rounds=10, runs_per_round=100_000, adam_steps=10, lr=1e-2,
-                        max_rows=10_000_000)
+    prop, log = P.train(net, q, seed=1, **IS_CE)
     train_s = time.perf_counter() - t0
     # importance sampling until the 95% CI half-width is 10% of the estimate
-    chunk = 100_000
+    chunk = IS_CHUNK
     s1 = s2 = 0.0
     n = 0
     t1 = time.perf_counter()
@@ -498,8 +501,8 @@ def run_rare_is(args):
             "value": train_s + is_s, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16 network / f32 accumulation / f64 log-weights", "data": "synthetic",
-            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1})", "ce_rounds": 10,
-                       "runs_per_round": 100_000},
+            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1})", "ce": IS_CE,
+                       "sample_chunk": chunk, "inference": "cuda cores (oracle order)"},
             "is": {"estimate": p, "ci_half": half, "runs": n, "train_s": train_s, "sample_s": is_s},
             "plain": {"estimate": p_plain, "ci_half": half_plain, "runs": plain_n, "runs_per_s": plain_rate,
                       "runs_for_10pct": need_plain, "seconds_for_10pct": plain_to_10},

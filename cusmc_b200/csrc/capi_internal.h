@@ -40,7 +40,7 @@ struct csmc_net {
     double *d_wvals = nullptr;         // per run: flag * likelihood ratio
     uint8_t *d_is_flags = nullptr;
     uint64_t is_cap = 0;
-    bool is_tc = true;  // importance sampling: theta by tensor cores (false: the oracle-identical evaluation)
+    bool is_tc = false;  // importance sampling: theta by warp-level MMAs (false: the oracle-identical CUDA-core evaluation)
 };
 
 namespace csmc {

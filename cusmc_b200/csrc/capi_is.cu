@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -53,29 +54,36 @@ int ensure_is_buffers(csmc_net *n, uint64_t runs) {
 }
 
 struct Launch {
-    int grid = 0, block = 128;
+    int grid = 0, block = CSMC_IS_BLOCK;
     size_t smem = 0;
+    uint32_t slab = 0;  // shared-memory bytes per warp (one run)
     bool slots = false, loc8 = false;
 };
 
+// One run per warp: the network and the proposal network once per CTA, then
+// one slab per warp; CTAs of fewer warps when the slabs do not fit.
 int plan_is(const csmc_net *n, bool trace, uint64_t n_runs, Launch &L) {
     const csmc_net_header &h = n->h;
     L.slots = h.max_edges_per_loc >= 2;
     L.loc8 = h.max_locs_per_comp <= 256;
     const size_t per = csmc::serial_state_bytes_per_thread(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, L.loc8);
-    L.smem = n->bytes + csmc::is_mlp_smem_bytes() + (n->is_tc ? csmc::is_stage_bytes(L.block) : 0) +
-             ((per * L.block + 15) & ~static_cast<size_t>(15));
+    L.slab = static_cast<uint32_t>(csmc::is_warp_slab_bytes(per, n->is_tc));
+    const size_t base = n->bytes + csmc::is_mlp_smem_bytes();
     int max_smem = 0, sms = 0, ctas = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device), "device attribute");
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device), "device attribute");
+    int warps = CSMC_IS_BLOCK / 32;
+    while (warps > 1 && base + static_cast<size_t>(warps) * L.slab > static_cast<size_t>(max_smem)) warps /= 2;
+    L.block = 32 * warps;
+    L.smem = base + static_cast<size_t>(warps) * L.slab;
     if (L.smem > static_cast<size_t>(max_smem))
-        return fail(CSMC_ERR_LIMIT, "importance sampling needs the network, the proposal network and the run state "
-                                    "of 128 runs in shared memory (" + std::to_string(L.smem) + " bytes)");
+        return fail(CSMC_ERR_LIMIT, "importance sampling needs the network, the proposal network and one run's "
+                                    "state in shared memory (" + std::to_string(L.smem) + " bytes)");
     int rc = csmc::is_max_active_ctas(n->is_tc, trace, L.slots, L.loc8, L.block, L.smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "importance-sampling kernel cannot be resident");
     uint64_t grid = static_cast<uint64_t>(sms) * ctas;
-    const uint64_t needed = (n_runs + L.block - 1) / L.block;
+    const uint64_t needed = (n_runs + warps - 1) / warps;
     if (grid > needed) grid = needed;
     L.grid = static_cast<int>(grid);
     return CSMC_OK;
@@ -129,9 +137,9 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
         return fail(CSMC_ERR_ARG, "run range out of bounds");
     std::memset(out, 0, sizeof *out);
     out->runs = n_runs;
-    out->lanes_per_run = 1;
-    out->comps_per_lane = static_cast<int32_t>(n->h.n_comps);
-    out->runs_per_cta = 128;
+    out->lanes_per_run = 32;
+    out->comps_per_lane = static_cast<int32_t>((n->h.n_comps + 31) / 32);
+    out->runs_per_cta = CSMC_IS_BLOCK / 32;
     out->family = 3;
     if (n_runs == 0) return CSMC_OK;
     CK(cudaSetDevice(n->device), "cudaSetDevice");
@@ -143,7 +151,9 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     CK(cudaMemcpyAsync(n->d_mlp, params, sizeof(csmc::MlpParams), cudaMemcpyHostToDevice, st), "upload proposal");
     CK(cudaMemsetAsync(n->d_scratch, 0, CSMC_SCRATCH_WORDS * sizeof(unsigned long long), st), "cudaMemsetAsync");
+    out->runs_per_cta = L.block / 32;
     csmc::IsParams ip = base_params(n, q, seed, first_run, n_runs);
+    ip.slab_bytes = L.slab;
     ip.s.flags = flags ? flags : n->d_is_flags;
     ip.s.values = values;
     ip.s.steps = steps;
@@ -191,6 +201,7 @@ int csmc_is_trace(csmc_net *n, const csmc_query *q, const void *params, uint64_t
     CK(cudaMemcpyAsync(n->d_mlp, params, sizeof(csmc::MlpParams), cudaMemcpyHostToDevice, st), "upload proposal");
     CK(cudaMemsetAsync(n->d_scratch, 0, CSMC_SCRATCH_WORDS * sizeof(unsigned long long), st), "cudaMemsetAsync");
     csmc::IsParams ip = base_params(n, q, seed, first_run, n_list);
+    ip.slab_bytes = L.slab;
     ip.trace_runs = runs;
     ip.trace_w = weights;
     ip.row_offset = row_offset;
@@ -205,12 +216,83 @@ int csmc_is_trace(csmc_net *n, const csmc_query *q, const void *params, uint64_t
 
 namespace {
 
-struct MlpScratch {  // per call, stream-ordered
+constexpr int kGradFloats = CSMC_MLP_HID * CSMC_MLP_IN + CSMC_MLP_HID * CSMC_MLP_HID + 3 * CSMC_MLP_HID + 1;
+static_assert(kGradFloats == CSMC_MLP_GRAD_FLOATS, "gradient layout of include/csmc.h");
+
+// Sums the per-CTA gradient partials of mlp_tc_kernel<1> into the gradient
+// (layout w1[64][16], b1[64], w2[64][64], b2[64], w3[64], b3; one thread per
+// entry, CTAs in order, FP64) and the per-CTA objectives into J.  A CTA's
+// partial block holds D4 = [dZ2 | dZ1]^T . [H1 | X | 1] (128 rows of 96:
+// row k < 64 is output unit k of layer 2, row 64 + j is unit j of layer 1;
+// columns 0..63 H1, 64..79 X, 80 the bias input), then dw3[64] and db3.
+__global__ void reduce_mlp_partials(const float *partials, const double *objective, int grid, int pf, float *grad,
+                                    double *J) {
+    constexpr int H = CSMC_MLP_HID, I = CSMC_MLP_IN, N4 = 96;
+    const int k = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k < kGradFloats) {
+        int src;
+        if (k < H * I) src = (64 + k / I) * N4 + 64 + k % I;                       // dW1[j][i]
+        else if (k < H * I + H) src = (64 + (k - H * I)) * N4 + 80;               // db1[j]
+        else if (k < H * I + H + H * H) src = ((k - H * I - H) / H) * N4 + (k - H * I - H) % H;  // dW2[k][j]
+        else if (k < H * I + 2 * H + H * H) src = (k - H * I - H - H * H) * N4 + 80;             // db2[k]
+        else if (k < H * I + 3 * H + H * H) src = 128 * N4 + (k - H * I - 2 * H - H * H);        // dw3[k]
+        else src = 128 * N4 + 64;                                                                // db3
+        double acc = 0.0;
+        for (int c = 0; c < grid; ++c) acc = csmc::d_add(acc, static_cast<double>(partials[c * pf + src]));
+        grad[k] = static_cast<float>(acc);
+    }
+    if (k == 0) {
+        double s = 0.0;
+        for (int c = 0; c < grid; ++c) s = csmc::d_add(s, objective[c]);
+        *J = s;
+    }
+}
+
+// Device buffers of the proposal-network kernels, one set per device, kept
+// for the life of the process (allocating per call would hand the memory
+// back to the driver at every synchronisation); a call holds the set's lock
+// until its stream has drained.
+struct MlpDevScratch {
+    std::mutex mu;
     csmc::MlpParams *P = nullptr;
     float *partials = nullptr;
     double *objective = nullptr;
     int *error = nullptr;
+    float *grad = nullptr;
+    double *J = nullptr;
+    int grid_cap = 0;
 };
+
+MlpDevScratch &mlp_scratch(int dev) {
+    static MlpDevScratch sets[64];
+    return sets[dev & 63];
+}
+
+int mlp_scratch_ensure(MlpDevScratch &m, int grid) {
+    if (m.P && grid <= m.grid_cap) return CSMC_OK;
+    cudaFree(m.P);
+    cudaFree(m.partials);
+    cudaFree(m.objective);
+    cudaFree(m.error);
+    cudaFree(m.grad);
+    cudaFree(m.J);
+    m.P = nullptr;
+    m.partials = nullptr;
+    m.objective = nullptr;
+    m.error = nullptr;
+    m.grad = nullptr;
+    m.J = nullptr;
+    m.grid_cap = 0;
+    const size_t pf = static_cast<size_t>(csmc::mlp_tc_partial_floats());
+    CK(cudaMalloc(&m.P, sizeof(csmc::MlpParams)), "cudaMalloc(proposal network)");
+    CK(cudaMalloc(&m.partials, grid * pf * sizeof(float)), "cudaMalloc(gradient partials)");
+    CK(cudaMalloc(&m.objective, grid * sizeof(double)), "cudaMalloc(objective partials)");
+    CK(cudaMalloc(&m.error, sizeof(int)), "cudaMalloc(error flag)");
+    CK(cudaMalloc(&m.grad, kGradFloats * sizeof(float)), "cudaMalloc(gradient)");
+    CK(cudaMalloc(&m.J, sizeof(double)), "cudaMalloc(objective)");
+    m.grid_cap = grid;
+    return CSMC_OK;
+}
 
 int mlp_common(int mode, const void *params, const void *rows, uint64_t n_rows, float *theta, float *grad,
                double *objective, void *stream) {
@@ -220,56 +302,30 @@ int mlp_common(int mode, const void *params, const void *rows, uint64_t n_rows, 
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
     const uint64_t tiles = (n_rows + 127) / 128;
     const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, sms)));
-    const size_t pf = static_cast<size_t>(csmc::mlp_tc_partial_floats());
+    const int pf = csmc::mlp_tc_partial_floats();
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    MlpScratch m;
-    CK(cudaMallocAsync(&m.P, sizeof(csmc::MlpParams), st), "cudaMallocAsync");
-    CK(cudaMallocAsync(&m.partials, grid * pf * sizeof(float), st), "cudaMallocAsync");
-    CK(cudaMallocAsync(&m.objective, grid * sizeof(double), st), "cudaMallocAsync");
-    CK(cudaMallocAsync(&m.error, sizeof(int), st), "cudaMallocAsync");
+    MlpDevScratch &m = mlp_scratch(dev);
+    std::lock_guard<std::mutex> lock(m.mu);
+    int rc = mlp_scratch_ensure(m, sms);
+    if (rc) return rc;
     CK(cudaMemsetAsync(m.error, 0, sizeof(int), st), "cudaMemsetAsync");
     CK(cudaMemcpyAsync(m.P, params, sizeof(csmc::MlpParams), cudaMemcpyHostToDevice, st), "upload proposal");
-    int rc = csmc::mlp_tc_launch(mode, static_cast<const csmc::MlpRow *>(rows), n_rows, m.P, theta, m.partials,
-                                 m.objective, m.error, grid, st);
+    rc = csmc::mlp_tc_launch(mode, static_cast<const csmc::MlpRow *>(rows), n_rows, m.P, theta, m.partials,
+                             m.objective, m.error, grid, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "tensor-core kernel launch");
     int err = 0;
-    std::vector<float> part(mode == 1 ? grid * pf : 0);
-    std::vector<double> obj(mode == 1 ? grid : 0);
+    double J = 0.0;
     CK(cudaMemcpyAsync(&err, m.error, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     if (mode == 1) {
-        CK(cudaMemcpyAsync(part.data(), m.partials, part.size() * sizeof(float), cudaMemcpyDeviceToHost, st),
-           "cudaMemcpyAsync");
-        CK(cudaMemcpyAsync(obj.data(), m.objective, obj.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
-           "cudaMemcpyAsync");
+        reduce_mlp_partials<<<(kGradFloats + 255) / 256, 256, 0, st>>>(m.partials, m.objective, grid, pf, m.grad,
+                                                                        m.J);
+        CK(cudaGetLastError(), "gradient reduction launch");
+        CK(cudaMemcpyAsync(grad, m.grad, kGradFloats * sizeof(float), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        CK(cudaMemcpyAsync(&J, m.J, sizeof(double), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     }
-    cudaFreeAsync(m.P, st);
-    cudaFreeAsync(m.partials, st);
-    cudaFreeAsync(m.objective, st);
-    cudaFreeAsync(m.error, st);
     CK(cudaStreamSynchronize(st), "tensor-core kernel");
     if (err) return fail(CSMC_ERR_TIMEOUT, "tensor-core kernel: a bounded wait for the MMA units gave up");
-    if (mode == 1) {
-        // gradient layout: w1[64][16], b1[64], w2[64][64], b2[64], w3[64], b3
-        constexpr int H = CSMC_MLP_HID, I = CSMC_MLP_IN, N4 = 96;
-        std::vector<double> acc(H * I + H + H * H + H + H + 1, 0.0);
-        double J = 0.0;
-        for (int c = 0; c < grid; ++c) {
-            const float *q = part.data() + c * pf;
-            for (int k = 0; k < H; ++k) {
-                for (int j = 0; j < H; ++j) acc[H * I + H + k * H + j] += q[k * N4 + j];  // dW2[k][j]
-                acc[H * I + H + H * H + k] += q[k * N4 + 80];                             // db2[k]
-            }
-            for (int j = 0; j < H; ++j) {
-                for (int i = 0; i < I; ++i) acc[j * I + i] += q[(64 + j) * N4 + 64 + i];  // dW1[j][i]
-                acc[H * I + j] += q[(64 + j) * N4 + 80];                                // db1[j]
-            }
-            for (int k = 0; k < H; ++k) acc[H * I + H + H * H + H + k] += q[128 * N4 + k];  // dw3[k]
-            acc[H * I + H + H * H + H + H] += q[128 * N4 + 64];                            // db3
-            J += obj[c];
-        }
-        for (size_t i = 0; i < acc.size(); ++i) grad[i] = static_cast<float>(acc[i]);
-        if (objective) *objective = J;
-    }
+    if (mode == 1 && objective) *objective = J;
     return CSMC_OK;
 }
 

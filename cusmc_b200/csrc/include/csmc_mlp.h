@@ -127,8 +127,42 @@ CSMC_HD void mlp_features(uint32_t l, const float *v, uint32_t n_int, uint32_t C
     x[9] = bf16_round(f_div(t, T));
 }
 
+/* Sums in the order of a 32-lane warp.  A run is simulated by one warp:
+ * component c belongs to lane (c / 4) mod 32 (the lane that draws its
+ * Philox block), each lane sums its own terms in component order, and the
+ * lanes' partial sums meet in a butterfly (offsets 16, 8, 4, 2, 1; lane L
+ * adds lane L ^ off's value to its own, so every lane ends with the same
+ * bits).  The CPU restatement keeps the 32 partial sums in an array. */
+#define CSMC_WARP 32
+CSMC_HD uint32_t warp_lane_of(uint32_t c) { return (c >> 2) & (CSMC_WARP - 1u); }
+static_assert(CSMC_MLP_HID == 2 * CSMC_WARP, "each lane holds two hidden units");
+
+CSMC_HD double warp_tree_d(double *p) {
+    for (uint32_t off = CSMC_WARP / 2; off > 0; off >>= 1) {
+        double q[CSMC_WARP];
+        for (uint32_t l = 0; l < CSMC_WARP; ++l) q[l] = d_add(p[l], p[l ^ off]);
+        for (uint32_t l = 0; l < CSMC_WARP; ++l) p[l] = q[l];
+    }
+    return p[0];
+}
+
+CSMC_HD float warp_tree_f(float *p) {
+    for (uint32_t off = CSMC_WARP / 2; off > 0; off >>= 1) {
+        float q[CSMC_WARP];
+        for (uint32_t l = 0; l < CSMC_WARP; ++l) q[l] = f_add(p[l], p[l ^ off]);
+        for (uint32_t l = 0; l < CSMC_WARP; ++l) p[l] = q[l];
+    }
+    return p[0];
+}
+
+CSMC_HD float clip_theta(float th) {
+    return th < -CSMC_MLP_THETA_MAX ? -CSMC_MLP_THETA_MAX : (th > CSMC_MLP_THETA_MAX ? CSMC_MLP_THETA_MAX : th);
+}
+
 /* theta for one feature row: first layer and GELU, activations rounded to
- * BF16, second layer and GELU, output dot product, clip. */
+ * BF16, second layer and GELU (each unit's dot product in input order),
+ * output layer in warp order (lane L: units L and L + 32, then the
+ * butterfly), plus the output bias, clipped. */
 CSMC_HD float mlp_theta(const MlpParams &P, const float *x) {
     float h1[CSMC_MLP_HID];
     for (int j = 0; j < CSMC_MLP_HID; ++j) {
@@ -136,13 +170,16 @@ CSMC_HD float mlp_theta(const MlpParams &P, const float *x) {
         for (int i = 0; i < CSMC_MLP_IN; ++i) z = f_fma(x[i], bf16_to_f(P.w1[j][i]), z);
         h1[j] = bf16_round(gelu_f(z));
     }
-    float th = P.b3;
+    float g[CSMC_MLP_HID];
     for (int k = 0; k < CSMC_MLP_HID; ++k) {
         float z = P.b2[k];
         for (int j = 0; j < CSMC_MLP_HID; ++j) z = f_fma(h1[j], bf16_to_f(P.w2[k][j]), z);
-        th = f_fma(gelu_f(z), P.w3[k], th);
+        g[k] = gelu_f(z);
     }
-    return th < -CSMC_MLP_THETA_MAX ? -CSMC_MLP_THETA_MAX : (th > CSMC_MLP_THETA_MAX ? CSMC_MLP_THETA_MAX : th);
+    float part[CSMC_WARP];
+    for (int l = 0; l < CSMC_WARP; ++l)
+        part[l] = f_fma(g[l + CSMC_WARP], P.w3[l + CSMC_WARP], f_fma(g[l], P.w3[l], 0.0f));
+    return clip_theta(f_add(P.b3, warp_tree_f(part)));
 }
 
 /* Multiplier of 1/rate under the proposal: e^(-theta). */

@@ -137,8 +137,8 @@ inline size_t batch_state_bytes_per_thread(uint32_t max_comps, uint32_t max_vars
 }
 
 // ---- Importance sampling (sim_is.cuh) --------------------------------------
-// The thread-per-run kernel under the proposal network; trace mode replays
-// listed runs and writes their CE training rows.
+// One warp per run under the proposal network; trace mode replays listed
+// runs and writes their CE training rows.
 struct IsParams {
     SimParams s;                  // network, query, run range; s.values: tracked values
     const MlpParams *mlp;         // proposal network (device)
@@ -148,6 +148,8 @@ struct IsParams {
     const float *trace_w;         // trace mode: CE weight per listed run
     const uint64_t *row_offset;   // trace mode: first row of each listed run (4 rows per step)
     MlpRow *rows;                 // trace mode: the rows
+    uint32_t slab_bytes;          // shared memory of one warp (is_warp_slab_bytes)
+    uint32_t pad;
 };
 
 // tc: theta by warp-level tensor-core MMAs (else the CUDA-core evaluation
@@ -155,11 +157,15 @@ struct IsParams {
 int is_launch(bool tc, bool trace, bool slots, bool loc8, const IsParams &p, int grid, int block, size_t smem,
               void *stream);
 int is_max_active_ctas(bool tc, bool trace, bool slots, bool loc8, int block, size_t smem, int *ctas);
-// Shared memory of the importance-sampling kernels besides network and
-// state: the proposal network, and (tensor-core kernel) each warp's staging
-// area of 128 feature rows.
+// Shared memory of the importance-sampling kernel besides the network: the
+// proposal network once per CTA, then one slab per warp holding the run's
+// state (the thread-per-run layout with one thread) and, for the CUDA-core
+// evaluation, the first hidden layer of the step's four rows.
 size_t is_mlp_smem_bytes();
-__host__ __device__ inline size_t is_stage_bytes(uint32_t threads) { return static_cast<size_t>(threads / 32) * 128 * 8 * 4; }
+#define CSMC_IS_BLOCK 256  // threads per CTA of the importance-sampling kernel (eight runs)
+inline size_t is_warp_slab_bytes(size_t run_state_bytes, bool tc) {
+    return (tc ? 0u : 4u * CSMC_MLP_HID * CSMC_MLP_CLASSES) + ((run_state_bytes + 15u) & ~static_cast<size_t>(15));
+}
 
 // Tensor-core kernels of the proposal network (mlp_train.cu): mode 0 writes
 // theta per row, mode 1 gradient partials per CTA (mlp_tc_partial_floats()

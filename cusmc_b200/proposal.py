@@ -118,8 +118,9 @@ def _ptr(t) -> int | None:
 
 
 def set_inference(net, tensor_cores: bool) -> None:
-    """Tensor-core evaluation of the proposal (default) or the CUDA-core one
-    that reproduces the CPU oracle bit for bit."""
+    """Warp-level tensor-core evaluation of the proposal, or the CUDA-core one
+    (the default: faster for the four rows a step evaluates) that reproduces
+    the CPU oracle bit for bit."""
     check(lib().csmc_is_set_inference(net._h, 1 if tensor_cores else 0))
 
 
@@ -184,10 +185,14 @@ def estimate(net, query: Query, proposal: Proposal | None, seed: int, n_runs: in
 
 def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: int = 100_000, rho: float = 0.1,
           adam_steps: int = 30, lr: float = 3e-3, init_seed: int = 0, max_rows: int = 40_000_000,
-          verbose: bool = False):
+          settle: int = 0, verbose: bool = False):
     """CE training of the proposal on the GPU.  The goal is the query's
-    threshold event (tracked value > threshold for a max query).  Returns
-    (Proposal, TrainLog)."""
+    threshold event (tracked value > threshold for a max query).  With
+    settle > 0 training stops after that many rounds whose level was the
+    goal itself (at least rho of the round's runs reached it).  Returns
+    (Proposal, TrainLog); each round's entry has its level, elite count,
+    rows, J before and after the Adam steps, and the seconds spent
+    simulating, replaying and in the gradient steps."""
     import torch
     dev = torch.device("cuda")
     prop = Proposal.init(init_seed)
@@ -200,6 +205,7 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
     values = torch.empty(n, dtype=torch.float64, device=dev)
     steps = torch.empty(n, dtype=torch.int32, device=dev)
     goal = query.threshold
+    at_goal = 0
     for k in range(rounds):
         t0 = time.perf_counter()
         params = prop.pack()
@@ -228,7 +234,10 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
         t_runs = torch.from_numpy(elite.astype(np.uint64).view(np.int64)).to(dev)
         t_w = torch.from_numpy(w).to(dev)
         t_off = torch.from_numpy(offs.view(np.int64)).to(dev)
+        t1 = time.perf_counter()
         is_trace(net, query, params, seed, t_runs, t_w, t_off, rows, first)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
         J0 = None
         for _ in range(adam_steps):
             g, J = mlp_grad(prop.pack(), rows, n_rows)
@@ -236,11 +245,17 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
                 J0 = J
             x = opt.ascend(x, g)
             prop = Proposal.from_vector(x)
+        t3 = time.perf_counter()
         hit_est = float(res.estimate)
         entry = {"round": k, "level": level, "elite": int(len(elite)), "rows": n_rows, "J_start": J0, "J_end": J,
-                 "estimate": hit_est, "hits": int(res.hits), "seconds": time.perf_counter() - t0}
+                 "estimate": hit_est, "hits": int(res.hits), "mean_steps": res.steps / max(res.runs, 1),
+                 "capped": int(res.capped), "kernel_ms": res.kernel_ms, "run_s": t1 - t0, "trace_s": t2 - t1,
+                 "adam_s": t3 - t2, "seconds": t3 - t0}
         log.rounds.append(entry)
         if verbose:
             print(entry, flush=True)
         del rows
+        at_goal = at_goal + 1 if level > goal else 0
+        if settle and at_goal >= settle:
+            break
     return prop, log

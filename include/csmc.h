@@ -237,10 +237,12 @@ void csmc_batch_free(csmc_batch *b);
  * csmc_mlp.h (CSMC_MLP_PARAM_BYTES bytes). */
 #define CSMC_MLP_PARAM_BYTES 11024
 
-/* How runs under the proposal evaluate theta (default 1): 1 = warp-level
- * BF16 tensor-core MMAs with FP32 accumulation; 0 = CUDA cores in the CPU
- * oracle's operation order (bit-identical runs).  Weights and estimates are
- * exact for the theta a run used either way. */
+/* How runs under the proposal evaluate theta (default 0): 0 = CUDA cores in
+ * the CPU oracle's operation order (bit-identical runs); 1 = warp-level BF16
+ * tensor-core MMAs with FP32 accumulation.  A run is one warp and a step
+ * evaluates four feature rows, too few to keep an MMA tile busy, so the
+ * CUDA-core evaluation is the faster one.  Weights and estimates are exact
+ * for the theta a run used either way. */
 int csmc_is_set_inference(csmc_net *net, int32_t tensor_cores);
 
 /* Runs first_run .. first_run+n_runs-1 under the proposal.  Per-run device
@@ -267,7 +269,10 @@ int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, floa
 /* Tensor-core gradient of J = sum over rows of (b theta - a e^theta) with
  * respect to the parameters (host floats, CSMC_MLP_GRAD_FLOATS of them:
  * w1[64][16], b1[64], w2[64][64], b2[64], w3[64], b3); *objective = J.
- * BF16 operands, FP32 accumulation in tensor memory. */
+ * BF16 operands, FP32 accumulation in tensor memory; the per-CTA partial
+ * sums are reduced on the device.  The two tensor-core entry points keep a
+ * small set of device buffers per device for the life of the process and
+ * serialise calls on the same device. */
 #define CSMC_MLP_GRAD_FLOATS 5313
 int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
                   void *stream);

@@ -374,21 +374,26 @@ class Run {
             const uint32_t win = idx[0];
             const float dmin = d[win];
             const bool finite = static_cast<double>(dmin) < kDblMax;
+            // sums over components in warp order (csmc_mlp.h: warp_lane_of,
+            // warp_tree_d), the order of the GPU kernel's one-warp-per-run step
             if (mlp_ && finite) {
-                double sum = 0.0;
+                double part[CSMC_WARP] = {};
                 for (uint32_t c = 0; c < C; ++c)
-                    if (tilted[c]) sum = d_add(sum, rate_change(inv[c], invp[c]));
+                    if (tilted[c]) part[warp_lane_of(c)] = d_add(part[warp_lane_of(c)], rate_change(inv[c], invp[c]));
+                const double sum = warp_tree_d(part);
                 logw_ = d_add(logw_, step_log_ratio(sum, dmin, tilted[win] != 0, inv[win], invp[win]));
             }
             if (mlp_ && rows_) {  // four rows per step, zero-weighted where nothing is tilted
                 for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) {
-                    double inv_sum = 0.0;
+                    double part[CSMC_WARP] = {};
                     uint32_t count = 0;
                     for (uint32_t c = 0; c < C; ++c)
                         if (tilted[c] && (loc_[c] & 3u) == l) {
-                            inv_sum = d_add(inv_sum, d_div(1.0, static_cast<double>(inv[c])));
+                            part[warp_lane_of(c)] =
+                                d_add(part[warp_lane_of(c)], d_div(1.0, static_cast<double>(inv[c])));
                             ++count;
                         }
+                    const double inv_sum = warp_tree_d(part);
                     const bool has = finite && count > 0;
                     MlpRow r;
                     for (int i = 0; i < CSMC_MLP_IN; ++i) r.x[i] = f_to_bf16(feat[l][i]);
