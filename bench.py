@@ -2,14 +2,17 @@
 epidemic network, Pr[<=100](<> R >= 50), 1,000,000 runs per step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload epidemic_100|random_0|mutex_8|mutex_32|mutex_64|mutex_256|batch_64|rare_is]
+                  [--workload epidemic_100|random_0|mutex_8|mutex_32|mutex_64|mutex_256|batch_64|rare_is|
+                              is_kernel|mlp_grad]
 
 The default workload is the epidemic; the others (the small random network
 and the Fischer-style mutex at n = 8, 32, 64, 256) use the same measurement
 with their own run counts (1e4 and 1e7 runs per step).  batch_64 times 64
 random networks in one graph-captured persistent launch against 64
 sequential launches; rare_is times learned importance sampling (CE training
-included) to a 10%-relative-error interval against plain SMC's rate.
+included) to a 10%-relative-error interval against plain SMC's rate;
+is_kernel times the importance-sampling kernel alone under the trained
+proposal, mlp_grad the tensor-core CE gradient on synthetic rows.
 
 A step is one pass of the hot path over one batch: 1e6 independent runs of
 the epidemic network (seeded synthetic input: the network comes from
@@ -514,6 +517,43 @@ def run_rare_is(args):
         print(json.dumps(line))
 
 
+def run_is_kernel(args):
+    """The importance-sampling kernel alone: trains the rare_is proposal
+    (IS_CE), then times csmc_is_run over --runs runs (default 1e5) per step
+    by the CUDA events the call records around its kernel launch.  Kernel
+    launches before the timed ones: two per CE round (runs, replay)."""
+    import torch
+    from cusmc_b200 import api, netgen, proposal as P
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    w = netgen.epidemic()
+    net = api.Network(_blob_of(w))
+    T, thr = IS_RARE
+    q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
+    prop, log = P.train(net, q, seed=1, **IS_CE)
+    params = prop.pack()
+    n = args.runs or 100_000
+    for i in range(args.warmup):
+        P.is_run(net, q, params, 9, n, 5_000_000_000 + i * n)
+    ms = []
+    steps = 0
+    for i in range(args.steps):
+        r = P.is_run(net, q, params, 9, n, 6_000_000_000 + i * n)
+        ms.append(r.kernel_ms)
+        steps += r.steps
+    net.close()
+    t = sum(ms) / 1000.0
+    line = {"metric": "runs/s of the importance-sampling kernel under a trained proposal", "value": n * args.steps / t,
+            "unit": "runs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 network evaluation / f64 log-weights", "data": "synthetic",
+            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1}), {n} runs per step",
+                       "ce_rounds": len(log.rounds), "launches_before_timed": 2 * len(log.rounds) + args.warmup},
+            "run_steps_per_s": steps / t, "steps_per_run": steps / (n * args.steps)}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def run_mlp_grad(args):
     """The tcgen05 gradient kernel of the proposal network on a seeded
     synthetic row set shaped like the epidemic's training rows (one-hot class,
@@ -563,7 +603,8 @@ def run_mlp_grad(args):
             "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
                          "frac": tflops / peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops"
                          if os.path.exists(pk) else "fallback"},
-            "note": "time per call includes the parameter upload, partial-sum copy and allocation of the call"}
+            "note": "time per call includes the parameter upload, the device reduction of the per-CTA partial "
+                    "sums and the copy of the gradient to the host"}
     print(json.dumps(line))
 
 
@@ -579,7 +620,7 @@ def main():
                          "smaller values are for profiling captures)")
     ap.add_argument("--batch-divisor", type=int, default=0,
                     help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
-    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "mlp_grad"],
+    ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "is_kernel", "mlp_grad"],
                     help="network and query (default: the 100-agent epidemic)")
     args = ap.parse_args()
     if args.workload == "batch_64" and args.impl == "ours":
@@ -588,7 +629,9 @@ def main():
         return run_rare_is(args)
     if args.workload == "mlp_grad" and args.impl == "ours":
         return run_mlp_grad(args)
-    if args.workload in ("batch_64", "rare_is", "mlp_grad"):
+    if args.workload == "is_kernel" and args.impl == "ours":
+        return run_is_kernel(args)
+    if args.workload in ("batch_64", "rare_is", "is_kernel", "mlp_grad"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference simulates one model per process and has "
                           "no importance sampling; this workload has no reference arm"}))
         return

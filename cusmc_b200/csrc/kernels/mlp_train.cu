@@ -46,7 +46,8 @@ constexpr uint32_t kB4 = kA4 + 128 * 128 * 2;   // F^T         96 x 128 (feature
 constexpr uint32_t kGz1 = kB4 + kN4 * 128 * 2;  // GELU'(z1) per thread, interleaved: 64 x 128 floats
 constexpr uint32_t kGz2 = kGz1 + 64 * 128 * 4;  // GELU'(z2) per thread, interleaved: 64 x 128 floats
 constexpr uint32_t kMisc = kGz2 + 64 * 128 * 4;  // mbarrier, tmem address, biases, reductions
-constexpr uint32_t kMiscBytes = 2048;
+constexpr uint32_t kMiscBytes = 4096;
+constexpr uint32_t kRedStride = 68;             // per-warp output-layer sums: dw3 (64), db3, pad
 constexpr uint32_t kSmemBytes = kMisc + kMiscBytes;
 
 constexpr uint32_t kWaitLimit = 1u << 20;       // bounded mbarrier polls
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kMisc);
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(sm + kMisc + 8);
-    float *red = reinterpret_cast<float *>(sm + kMisc + 16);   // dw3 (64), db3
+    float *red = reinterpret_cast<float *>(sm + kMisc + 1536);  // [warp][kRedStride]: dw3 (64), db3
     float *b1s = reinterpret_cast<float *>(sm + kMisc + 512);
     float *b2s = reinterpret_cast<float *>(sm + kMisc + 768);
     float *w3s = reinterpret_cast<float *>(sm + kMisc + 1024);
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(128, 1)
         b2s[tid] = P->b2[tid];
         w3s[tid] = P->w3[tid];
     }
-    if (tid < 65) red[tid] = 0.0f;
+    for (uint32_t i = tid; i < 4 * kRedStride; i += blockDim.x) red[i] = 0.0f;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -269,17 +270,20 @@ __global__ void __launch_bounds__(128, 1)
         const float e = exp2_f(f_mul(thc, 1.44269502f));
         if (valid) J += static_cast<double>(row.b) * thc - static_cast<double>(row.a) * e;
         const float g = (valid && inside) ? f_add(row.b, -f_mul(row.a, e)) : 0.0f;
-        // output layer: dw3 += g h2, db3 += g (warp sums, then shared atomics)
+        // output layer: dw3 += g h2, db3 += g (warp sums into the warp's own
+        // slots; the four warps' slots are added in a fixed order at the end,
+        // so the gradient does not depend on warp timing)
+        float *rw = red + warp * kRedStride;
         float gs = g;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, o);
-        if (lane == 0) atomicAdd(&red[64], gs);
+        if (lane == 0) rw[64] += gs;
 #pragma unroll
         for (int k = 0; k < 64; ++k) {
             float v = f_mul(g, z2[k]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) atomicAdd(&red[k], v);
+            if (lane == 0) rw[k] += v;
             const float dz = f_mul(f_mul(g, w3s[k]), gz2[k * 128 + tid]);
             st_bf16(sm + kA3, kmaj(tid, k, kRows), dz);
             st_bf16(sm + kA4, kmaj(k, tid, kRows), dz);
@@ -344,7 +348,9 @@ __global__ void __launch_bounds__(128, 1)
             for (int i = 0; i < kN4; ++i) out[tid * kN4 + i] = 0.0f;
         }
         __syncthreads();
-        if (tid < 65) out[128 * kN4 + tid] = red[tid];
+        if (tid < 65)
+            out[128 * kN4 + tid] =
+                f_add(f_add(f_add(red[tid], red[kRedStride + tid]), red[2 * kRedStride + tid]), red[3 * kRedStride + tid]);
         if (tid == 65) out[128 * kN4 + 65] = 0.0f;
         __shared__ double jred[128];
         jred[tid] = J;

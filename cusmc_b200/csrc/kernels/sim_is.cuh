@@ -362,6 +362,9 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
 #pragma unroll
     for (int i = 0; i < CSMC_MLP_IN - 4; ++i) x_last[i] = 0xffffffffu;  // a NaN: never equal to a feature
     float mfac[CSMC_MLP_CLASSES] = {1.0f, 1.0f, 1.0f, 1.0f};
+    // the last tilted winner's 1/rate and 1/rate' bits and its log term
+    uint32_t w_inv = 0xffffffffu, w_invp = 0xffffffffu;
+    double w_term = 0.0;
 
     for (;;) {
         unsigned long long ridx = 0;
@@ -396,6 +399,10 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
         float time = 0.0f;
         uint32_t step = 0;
         double logw = 0.0;
+        // the rate table is a function of the variables: evaluated on a
+        // run's first step and after steps that can have changed a variable
+        // (a transition, a receiver, or clocks advancing)
+        bool stale = true;
         for (;;) {
             int done = 0;
             if (lane == 0) {
@@ -417,9 +424,11 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
             if (__shfl_sync(kFullWarp, done, 0)) break;
 
             // pending broadcast receivers (serial, lane 0), then the rate table
-            if (lane == 0) run_receivers<false, SLOTS, LOC8>(n, C, V, rv, sc, p.seed, p.var_id, run, step);
+            int moved = 0;
+            if (lane == 0) moved = run_receivers<false, SLOTS, LOC8>(n, C, V, rv, sc, p.seed, p.var_id, run, step);
             __syncwarp();
-            if (rate_table) {
+            stale = stale || __shfl_sync(kFullWarp, moved, 0) != 0;
+            if (rate_table && stale) {
                 for (uint32_t j = lane; j < P; j += 32u) rv.rates[j] = inv_rate(eval(n, rv.vars, n.rate_prog[j]));
                 __syncwarp();
             }
@@ -459,7 +468,21 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
             const bool tilted_w = __shfl_sync(kFullWarp, static_cast<int>(R.best_tilted), owner) != 0;
             const double rate_sum = warp_sum_d(R.rate_sum);
             const bool finite = static_cast<double>(dmin) < kDblMax;
-            if (finite) logw = d_add(logw, step_log_ratio(rate_sum, dmin, tilted_w, inv_w, invp_w));
+            if (finite) {
+                // step_log_ratio, with ln2 * log2(inv'_w / inv_w) of the last
+                // tilted winner's (1/rate, 1/rate') pair reused
+                const double ln2 = 0.6931471805599453;
+                double r = d_mul(d_mul(ln2, rate_sum), static_cast<double>(dmin));
+                if (tilted_w) {
+                    if (__float_as_uint(inv_w) != w_inv || __float_as_uint(invp_w) != w_invp) {
+                        w_inv = __float_as_uint(inv_w);
+                        w_invp = __float_as_uint(invp_w);
+                        w_term = d_mul(ln2, log2_d(d_div(static_cast<double>(invp_w), static_cast<double>(inv_w))));
+                    }
+                    r = d_add(r, w_term);
+                }
+                logw = d_add(logw, r);
+            }
             if (TRACE) {
                 double inv_sum[CSMC_MLP_CLASSES];
 #pragma unroll
@@ -480,12 +503,15 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
             }
 
             // the winner's transition (lane 0), then the time update
+            int took = 0;
             if (lane == 0) {
                 uint32_t s0 = step;
                 float t0 = time;
-                run_commit<false, SLOTS, LOC8>(n, p.net.n_clocks, rv, sc, p.seed, p.var_id, run, s0, t0, win, dmin);
+                took = run_commit<false, SLOTS, LOC8>(n, p.net.n_clocks, rv, sc, p.seed, p.var_id, run, s0, t0, win,
+                                                      dmin);
             }
             __syncwarp();
+            stale = __shfl_sync(kFullWarp, took, 0) != 0 || (p.net.n_clocks > 0 && finite);
             time = d2f(d_add(static_cast<double>(time), static_cast<double>(dmin)));
             ++step;
         }

@@ -126,13 +126,15 @@ static __device__ __forceinline__ void run_final_state(const Net &n, uint32_t C,
 // Pending broadcast receivers of the previous step's sender (SyncInSerial,
 // simulation.cu:357-407): enabled sets from the state the sender left (the
 // snapshot), then transitions in component order on the live state.
+// Returns true when a receiver took an edge.
 template <bool VERIFY, bool SLOTS, bool LOC8>
-static __device__ __forceinline__ void run_receivers(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+static __device__ __forceinline__ bool run_receivers(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
                                                      RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
                                                      uint32_t step) {
-    if (sc.chan <= 0) return;
+    if (sc.chan <= 0) return false;
     const uint32_t T = rv.T;
     const int chan = sc.chan, sender = sc.sender;
+    bool moved = false;
     if (has_receivers(n, chan)) {
         for (uint32_t v = 0; v < V; ++v) rv.shadow[v] = rv.vars[v];
         for (uint32_t c = 0; c < C; ++c) {
@@ -150,20 +152,24 @@ static __device__ __forceinline__ void run_receivers(const Net &n, uint32_t C, u
             const uint32_t base = n.comp[c].loc_begin;
             const uint32_t nl = take_edge<VERIFY>(n, rv.vars, sc, seed, var_id, run, step, c, li - base, m, sm, 1);
             rv.set_local(n, c, nl);
+            moved = true;
         }
     }
     sc.chan = 0;
     sc.sender = -1;
+    return moved;
 }
 
 // The race's outcome applied (simulation.cu:632-667, 876-882): clocks
 // advance by dmin, the winner takes an enabled edge, time advances.
+// Returns true when the winner took an edge.
 template <bool VERIFY, bool SLOTS, bool LOC8>
-static __device__ __forceinline__ void run_commit(const Net &n, uint32_t n_clocks, const RunView<LOC8> &rv,
+static __device__ __forceinline__ bool run_commit(const Net &n, uint32_t n_clocks, const RunView<LOC8> &rv,
                                                   RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
                                                   uint32_t &step, float &time, uint32_t win, float dmin) {
     const uint32_t T = rv.T;
     const VarView vars = rv.vars;
+    bool took = false;
     if (VERIFY) {
         mix(sc.digest, step);
         mix(sc.digest, win);
@@ -185,12 +191,14 @@ static __device__ __forceinline__ void run_commit(const Net &n, uint32_t n_clock
             const uint32_t base = n.comp[win].loc_begin;
             const uint32_t nl = take_edge<VERIFY>(n, vars, sc, seed, var_id, run, step, win, li - base, en, sm, 0);
             rv.set_local(n, win, nl);
+            took = true;
         } else if (VERIFY) {
             mix(sc.digest, 0xffffffffu);
         }
     }
     time = d2f(d_add(static_cast<double>(time), static_cast<double>(dmin)));
     ++step;
+    return took;
 }
 
 // The race over every component (simulation.cu:409-628): per-component
