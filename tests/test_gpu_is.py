@@ -48,6 +48,9 @@ def _random_proposal(seed, out_scale=0.3):
 
 CASES = {
     "epidemic": lambda: (netgen.epidemic(), 100, 49),
+    # 160 components: lanes 0..7 of the warp draw two Philox blocks each, so
+    # their partial sums span two blocks (the warp order of csmc_mlp.h)
+    "epidemic_160": lambda: (netgen.epidemic(n_agents=160), 60, 79),
     "random": lambda: (netgen.random_network(3), None, None),
     "mutex": lambda: (netgen.mutex(8), None, None),
 }
