@@ -183,17 +183,64 @@ def estimate(net, query: Query, proposal: Proposal | None, seed: int, n_runs: in
     return p, half, dev_s
 
 
+@dataclass
+class Elite:
+    """One CE round's training set: the level, the elite runs (indices into
+    the round), their normalised CE weights (float32), the first row of each
+    run's block in the row buffer (four rows per step) and the row count."""
+
+    level: float
+    runs: np.ndarray
+    weights: np.ndarray
+    row_offset: np.ndarray
+    n_rows: int
+    at_goal: bool
+
+
+def select_elite(values: np.ndarray, logw: np.ndarray, steps: np.ndarray, threshold: float, is_max: bool = True,
+                 rho: float = 0.1, max_rows: int = 40_000_000) -> Elite:
+    """Multi-level CE selection for the goal value > threshold (max query) or
+    value < threshold (min query): the level is the (1 - rho)-quantile of the
+    runs' scores (the value, negated for a min query), capped at the goal;
+    the elite are the runs at or beyond the level (strictly beyond the goal
+    once the level reaches it), weighted by their likelihood ratios.  Runs
+    are kept heaviest first while their rows (4 per step) fit in max_rows,
+    and at least one run is kept."""
+    score = np.asarray(values, np.float64) if is_max else -np.asarray(values, np.float64)
+    goal = threshold if is_max else -threshold
+    n = len(score)
+    level = min(goal + 1e-9, float(np.quantile(score, 1.0 - rho)))
+    elite = np.nonzero(score >= level)[0] if level <= goal else np.nonzero(score > goal)[0]
+    if len(elite) == 0:
+        elite = np.argsort(score)[-max(1, int(rho * n)):]
+    lw = np.asarray(logw, np.float64)[elite]
+    w = np.exp(lw - lw.max())
+    w = w / w.sum()
+    st = np.asarray(steps).astype(np.int64)
+    order = np.argsort(-w)
+    keep = order[np.cumsum(4 * st[elite][order]) <= max_rows]
+    if len(keep) == 0:
+        keep = order[:1]
+    elite, w = elite[keep], w[keep]
+    w = (w / w.sum()).astype(np.float32)
+    offs = np.concatenate([[0], np.cumsum(4 * st[elite])[:-1]]).astype(np.uint64)
+    return Elite(level if is_max else -level, elite, w, offs, int((4 * st[elite]).sum()), level > goal)
+
+
 def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: int = 100_000, rho: float = 0.1,
           adam_steps: int = 30, lr: float = 3e-3, init_seed: int = 0, max_rows: int = 40_000_000,
           settle: int = 0, verbose: bool = False):
     """CE training of the proposal on the GPU.  The goal is the query's
-    threshold event (tracked value > threshold for a max query).  With
-    settle > 0 training stops after that many rounds whose level was the
-    goal itself (at least rho of the round's runs reached it).  Returns
-    (Proposal, TrainLog); each round's entry has its level, elite count,
-    rows, J before and after the Adam steps, and the seconds spent
+    threshold event (tracked value > threshold for a max query, < threshold
+    for a min query; a location query has no value to rank runs by and is
+    refused).  With settle > 0 training stops after that many rounds whose
+    level was the goal itself (at least rho of the round's runs reached it).
+    Returns (Proposal, TrainLog); each round's entry has its level, elite
+    count, rows, J before and after the Adam steps, and the seconds spent
     simulating, replaying and in the gradient steps."""
     import torch
+    if query.kind != 1:
+        raise ValueError("CE training needs a variable query (the tracked value ranks the runs)")
     dev = torch.device("cuda")
     prop = Proposal.init(init_seed)
     x = prop.vector()
@@ -204,36 +251,19 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
     logw = torch.empty(n, dtype=torch.float64, device=dev)
     values = torch.empty(n, dtype=torch.float64, device=dev)
     steps = torch.empty(n, dtype=torch.int32, device=dev)
-    goal = query.threshold
     at_goal = 0
     for k in range(rounds):
         t0 = time.perf_counter()
         params = prop.pack()
         first = (k + 1) * 10_000_000  # each round uses fresh runs of the stream
         res = is_run(net, query, params, seed, n, first, flags=flags, logw=logw, values=values, steps=steps)
-        lw = logw.cpu().numpy()
-        val = values.cpu().numpy()
-        st = steps.cpu().numpy().view(np.uint32).astype(np.int64)
-        level = min(goal + 1e-9, float(np.quantile(val, 1.0 - rho)))
-        elite = np.nonzero(val >= level)[0] if level <= goal else np.nonzero(val > goal)[0]
-        if len(elite) == 0:
-            elite = np.argsort(val)[-max(1, int(rho * n)):]
-        w = np.exp(lw[elite] - lw[elite].max())
-        w = w / w.sum()
-        # cap the row set
-        order = np.argsort(-w)
-        rows_needed = 4 * st[elite]
-        keep = order[np.cumsum(rows_needed[order]) <= max_rows]
-        if len(keep) == 0:
-            keep = order[:1]
-        elite, w = elite[keep], w[keep]
-        w = (w / w.sum()).astype(np.float32)
-        offs = np.concatenate([[0], np.cumsum(4 * st[elite])[:-1]]).astype(np.uint64)
-        n_rows = int((4 * st[elite]).sum())
+        sel = select_elite(values.cpu().numpy(), logw.cpu().numpy(), steps.cpu().numpy().view(np.uint32),
+                           query.threshold, bool(query.is_max), rho, max_rows)
+        elite, n_rows = sel.runs, sel.n_rows
         rows = torch.empty(n_rows * ROW_BYTES, dtype=torch.uint8, device=dev)
         t_runs = torch.from_numpy(elite.astype(np.uint64).view(np.int64)).to(dev)
-        t_w = torch.from_numpy(w).to(dev)
-        t_off = torch.from_numpy(offs.view(np.int64)).to(dev)
+        t_w = torch.from_numpy(sel.weights).to(dev)
+        t_off = torch.from_numpy(sel.row_offset.view(np.int64)).to(dev)
         t1 = time.perf_counter()
         is_trace(net, query, params, seed, t_runs, t_w, t_off, rows, first)
         torch.cuda.synchronize()
@@ -247,7 +277,7 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
             prop = Proposal.from_vector(x)
         t3 = time.perf_counter()
         hit_est = float(res.estimate)
-        entry = {"round": k, "level": level, "elite": int(len(elite)), "rows": n_rows, "J_start": J0, "J_end": J,
+        entry = {"round": k, "level": sel.level, "elite": int(len(elite)), "rows": n_rows, "J_start": J0, "J_end": J,
                  "estimate": hit_est, "hits": int(res.hits), "mean_steps": res.steps / max(res.runs, 1),
                  "capped": int(res.capped), "kernel_ms": res.kernel_ms, "run_s": t1 - t0, "trace_s": t2 - t1,
                  "adam_s": t3 - t2, "seconds": t3 - t0}
@@ -255,7 +285,7 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
         if verbose:
             print(entry, flush=True)
         del rows
-        at_goal = at_goal + 1 if level > goal else 0
+        at_goal = at_goal + 1 if sel.at_goal else 0
         if settle and at_goal >= settle:
             break
     return prop, log
