@@ -130,7 +130,7 @@ _SIGNATURES = {
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),
     "csmc_is_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_char_p, ctypes.c_uint64,
                                      ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "csmc_mlp_forward": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                         ctypes.c_void_p]),
     "csmc_mlp_grad": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,

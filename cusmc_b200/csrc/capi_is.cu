@@ -186,7 +186,7 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
 
 int csmc_is_trace(csmc_net *n, const csmc_query *q, const void *params, uint64_t seed, uint64_t first_run,
                   const uint64_t *runs, const float *weights, const uint64_t *row_offset, uint64_t n_list, void *rows,
-                  void *stream) {
+                  uint64_t rows_cap, void *stream) {
     if (!n || !q || !params || !runs || !weights || !row_offset || !rows) return fail(CSMC_ERR_ARG, "null argument");
     int rc = check_query(n, q);
     if (rc) return rc;
@@ -206,9 +206,13 @@ int csmc_is_trace(csmc_net *n, const csmc_query *q, const void *params, uint64_t
     ip.trace_w = weights;
     ip.row_offset = row_offset;
     ip.rows = static_cast<csmc::MlpRow *>(rows);
+    ip.rows_cap = rows_cap;
     rc = csmc::is_launch(n->is_tc, true, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "replay kernel launch");
+    unsigned long long sc[CSMC_SCRATCH_WORDS];
+    CK(cudaMemcpyAsync(sc, n->d_scratch, sizeof sc, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     CK(cudaStreamSynchronize(st), "replay kernel");
+    if (sc[4]) return fail(CSMC_ERR_LIMIT, std::to_string(sc[4]) + " replay rows fall beyond the row buffer");
     return CSMC_OK;
 }
 

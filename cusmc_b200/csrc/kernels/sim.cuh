@@ -148,6 +148,7 @@ struct IsParams {
     const float *trace_w;         // trace mode: CE weight per listed run
     const uint64_t *row_offset;   // trace mode: first row of each listed run (4 rows per step)
     MlpRow *rows;                 // trace mode: the rows
+    uint64_t rows_cap;            // trace mode: rows the buffer holds (writes beyond it are skipped, counted)
     uint32_t slab_bytes;          // shared memory of one warp (is_warp_slab_bytes)
     uint32_t pad;
 };

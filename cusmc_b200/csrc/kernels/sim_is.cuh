@@ -373,11 +373,11 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
         if (ridx >= p.n_runs) break;
         uint64_t run;
         float row_w = 0.0f;
-        MlpRow *rows = nullptr;
+        uint64_t row0 = 0;  // replay: the run's first row in the buffer
         if (TRACE) {
             run = p.first_run + ip.trace_runs[ridx];
             row_w = ip.trace_w[ridx];
-            rows = ip.rows + ip.row_offset[ridx];
+            row0 = ip.row_offset[ridx];
         } else {
             run = p.first_run + ridx;
         }
@@ -498,7 +498,9 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
                     for (int i = 0; i < CSMC_MLP_IN; ++i) row.x[i] = f_to_bf16(feat_of(x, lane, i));
                     row.a = has ? row_a(s, dmin, row_w) : 0.0f;
                     row.b = (has && tilted_w && wl == lane) ? row_w : 0.0f;
-                    rows[4u * step + lane] = row;
+                    const uint64_t r = row0 + 4ull * step + lane;
+                    if (r < ip.rows_cap) ip.rows[r] = row;
+                    else atomicAdd(p.scratch + 4, 1ull);
                 }
             }
 

@@ -135,9 +135,11 @@ def is_run(net, query: Query, params: bytes, seed: int, n_runs: int, first_run: 
 
 def is_trace(net, query: Query, params: bytes, seed: int, runs, weights, row_offset, rows, first_run: int = 0,
              stream=None) -> None:
-    """csmc_is_trace: runs/weights/row_offset/rows are torch CUDA tensors."""
+    """csmc_is_trace: runs/weights/row_offset/rows are torch CUDA tensors
+    (rows: a byte buffer of whole 40-byte rows, its size the row capacity)."""
     check(lib().csmc_is_trace(net._h, ctypes.byref(query), params, seed & (2**64 - 1), first_run, _ptr(runs),
-                              _ptr(weights), _ptr(row_offset), len(runs), _ptr(rows), stream))
+                              _ptr(weights), _ptr(row_offset), len(runs), _ptr(rows),
+                              rows.numel() * rows.element_size() // ROW_BYTES, stream))
 
 
 def mlp_forward(params: bytes, rows, n_rows: int, theta, stream=None) -> None:

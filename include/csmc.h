@@ -257,10 +257,13 @@ int csmc_is_run(csmc_net *net, const csmc_query *q, const void *params, uint64_t
 /* Replays runs first_run + runs[i] (device list of n_list offsets) under the
  * proposal and writes their CE training rows (csmc::MlpRow, 40 bytes: BF16
  * features, a, b) to rows: four rows per step starting at row_offset[i]
- * (device), weighted by weights[i] (device). */
+ * (device), weighted by weights[i] (device).  rows holds rows_cap rows; a
+ * row that would land at or beyond rows_cap is not written and the call
+ * returns CSMC_ERR_LIMIT (offsets that do not match the runs' step counts
+ * under the same proposal and inference mode). */
 int csmc_is_trace(csmc_net *net, const csmc_query *q, const void *params, uint64_t seed, uint64_t first_run,
                   const uint64_t *runs, const float *weights, const uint64_t *row_offset, uint64_t n_list, void *rows,
-                  void *stream);
+                  uint64_t rows_cap, void *stream);
 
 /* Tensor-core (tcgen05) forward pass of the proposal network over n_rows
  * device rows (csmc::MlpRow): theta (device, n_rows floats, clipped). */
