@@ -46,6 +46,13 @@ double number(const std::string &f, const std::string &s) {
     return v;
 }
 
+// A number the query can use: finite (stod also reads "nan" and "inf").
+double finite_number(const std::string &f, const std::string &s, const char *what) {
+    const double v = number(f, s);
+    if (!std::isfinite(v)) bad(f, std::string(what) + " must be a finite number, not '" + s + "'");
+    return v;
+}
+
 int var_id(const Network &net, const std::string &f, const std::string &name) {
     for (size_t i = 0; i < net.var_names.size(); ++i)
         if (net.var_names[i] == name) return static_cast<int>(i);
@@ -101,12 +108,14 @@ QueryText parse_formula(const Network &net, const std::string &formula) {
     std::string bound = f.substr(lb + 3, rb - lb - 3);
     const size_t semi = bound.find(';');
     if (semi != std::string::npos) {
-        const double n = number(formula, bound.substr(semi + 1));
+        const double n = finite_number(formula, bound.substr(semi + 1), "the run count");
         if (!(n >= 1) || n != std::floor(n)) bad(formula, "the run count must be a positive integer");
+        if (n > 9007199254740992.0) bad(formula, "the run count must be at most 2^53");
         q.sims = static_cast<uint64_t>(n);
         bound = bound.substr(0, semi);
     }
-    q.horizon = number(formula, bound);
+    q.horizon = finite_number(formula, bound, "the time bound");
+    if (q.horizon < 0) bad(formula, "the time bound must not be negative");
     if (rb + 1 >= f.size() || f[rb + 1] != '(') bad(formula, "expected '(' after the bound");
     const size_t end = close(rb + 1);
     if (end != f.size() - 1) bad(formula, "unexpected text after the formula");
@@ -133,7 +142,7 @@ QueryText parse_formula(const Network &net, const std::string &formula) {
         const size_t p = body.find(op);
         if (p == std::string::npos) continue;
         const std::string lhs = body.substr(0, p), rhs = body.substr(p + std::string(op).size());
-        const double k = number(formula, rhs);
+        const double k = finite_number(formula, rhs, "the threshold");
         q.kind = 1;
         q.is_estimate = 0;
         q.var_id = var_id(net, formula, lhs);

@@ -47,6 +47,14 @@ def test_location_reachability_by_template_and_local_variables(tmp_path):
     ("Pr[<=10](<> P0.nowhere)", "no location"),
     ("E[<=10](max: id)", "run count"),
     ("Pr[<=10](<> id == 1)", "equality"),
+    ("Pr[<=nan](<> id >= 1)", "time bound must be a finite number"),
+    ("Pr[<=inf](<> id >= 1)", "time bound must be a finite number"),
+    ("Pr[<=-5](<> id >= 1)", "must not be negative"),
+    ("Pr[<=10](<> id >= nan)", "threshold must be a finite number"),
+    ("Pr[<=10; 0](<> id >= 1)", "positive integer"),
+    ("Pr[<=10; 2.5](<> id >= 1)", "positive integer"),
+    ("Pr[<=10; 99999999999999999999999](<> id >= 1)", "at most 2^53"),
+    ("Pr[<=1e400](<> id >= 1)", "not a number"),
 ])
 def test_unsupported_formulas_are_rejected(tmp_path, formula, msg):
     path = netgen.mutex(2).write(str(tmp_path / "m.xml"))
