@@ -237,3 +237,134 @@ def batch_networks(count: int = 64, base_seed: int = 1000):
         w.name = f"batch_{i}"
         out.append(w)
     return out
+
+
+def expression_zoo(seed: int, full: bool = False) -> Workload:
+    """A small random network that exercises the front end's expression
+    language: integer, double and constant operands, + - * / (and with full:
+    %, unary minus, sqrt(), random(), || and negated guards), comparisons and
+    conjunctions in guards, conditional assignments c ? a : b, clock guards
+    and invariants, exponential rates given as expressions, committed and
+    urgent locations, branchpoints with probability weights, broadcast
+    senders and receivers, local clocks and ints.  Every location lies on a
+    cycle through the template, so it is reachable.  Many full models fall
+    outside the subset the reference front end accepts; the front end must
+    then reject them as the reference does.  Query Pr[<=50](<> v0 >= 4)."""
+    rng = random.Random(seed)
+
+    def operand(ints, dbls):
+        r = rng.random()
+        if r < 0.45:
+            return rng.choice(ints)
+        if r < 0.6 and dbls:
+            return rng.choice(dbls)
+        if r < 0.85:
+            return str(rng.randint(0, 9))
+        return f"{rng.randint(0, 9)}.{rng.randint(0, 99)}"
+
+    def expr(depth, ints, dbls, cond_ok=False):
+        if depth <= 0 or rng.random() < 0.3:
+            return operand(ints, dbls)
+        k = rng.random()
+        if k < 0.55:
+            ops = ["+", "-", "*", "/", "%"] if full else ["+", "-", "*", "/"]
+            return f"({expr(depth - 1, ints, dbls)} {rng.choice(ops)} {expr(depth - 1, ints, dbls)})"
+        if full and k < 0.65:
+            return f"-{expr(depth - 1, ints, dbls)}"
+        if full and k < 0.75:
+            return f"sqrt({expr(depth - 1, ints, dbls)})"
+        if full and k < 0.8:
+            return f"random({rng.randint(1, 9)})"
+        if cond_ok and k < 0.9:
+            return f"{cond(depth - 1, ints, dbls)} ? {expr(depth - 1, ints, dbls)} : {expr(depth - 1, ints, dbls)}"
+        return f"({expr(depth - 1, ints, dbls)})"
+
+    def cond(depth, ints, dbls):
+        op = rng.choice(["<", "<=", ">", ">=", "==", "!="])
+        return f"{rng.choice(ints)} {op} {expr(max(0, depth - 1), ints, dbls)}"
+
+    def guard(ints, dbls, clocks):
+        parts = []
+        for _ in range(rng.randint(1, 3)):
+            if clocks and rng.random() < 0.4:
+                parts.append(f"{rng.choice(clocks)} {rng.choice(['>=', '>', '<=', '<'])} {rng.randint(0, 9)}")
+            else:
+                parts.append(cond(2, ints, dbls))
+        g = (rng.choice([" && ", " && ", " || "]) if full else " && ").join(parts)
+        if full and rng.random() < 0.1:
+            g = "!(" + g + ")"
+        return g
+
+    ints = [f"v{i}" for i in range(rng.randint(1, 4))]
+    dbls = [f"d{i}" for i in range(rng.randint(0, 2))]
+    consts = [f"K{i}" for i in range(rng.randint(0, 2))]
+    decl = [f"int {v} = {rng.randint(0, 5)};" for v in ints]
+    decl += [f"double {d} = {rng.randint(0, 5)}.{rng.randint(0, 9)};" for d in dbls]
+    decl += [f"const int {c} = {rng.randint(1, 9)};" for c in consts]
+    decl += ["broadcast chan b;"]
+    parts = ['<?xml version="1.0" encoding="utf-8"?>', "<nta>", f"<declaration>{escape(chr(10).join(decl))}</declaration>"]
+    counter = [0]
+
+    def new_id():
+        counter[0] += 1
+        return f"id{counter[0]}"
+
+    names = []
+    for t in range(rng.randint(1, 4)):
+        name = f"T{t}"
+        clocks = ["x"] if rng.random() < 0.7 else []
+        local = (["clock x;"] if clocks else []) + ([f"int w = {rng.randint(0, 3)};"] if rng.random() < 0.3 else [])
+        lints = ints + consts + (["w"] if any(s.startswith("int w") for s in local) else [])
+        n = rng.randint(2, 5)
+        ids = [new_id() for _ in range(n)]
+        parts += ["<template>", f"<name>{name}</name>", f"<declaration>{escape(chr(10).join(local))}</declaration>"]
+        for i, lid in enumerate(ids):
+            parts += [f'<location id="{lid}">', f"<name>L{i}</name>"]
+            r = rng.random()
+            if clocks and r < 0.25:
+                parts.append(_label("invariant", f"x <= {rng.randint(2, 9)}"))
+            elif r < 0.7:
+                rate = expr(2, lints, dbls) if rng.random() < 0.4 else str(rng.randint(1, 5))
+                parts.append(_label("exponentialrate", rate))
+            if rng.random() < 0.1:
+                parts.append("<committed/>")
+            elif rng.random() < 0.1:
+                parts.append("<urgent/>")
+            parts.append("</location>")
+        bp = new_id() if rng.random() < 0.4 else None
+        if bp:
+            parts.append(f'<branchpoint id="{bp}"/>')
+        parts.append(f'<init ref="{ids[0]}"/>')
+        for i in range(n):
+            outs = rng.randint(1, 3)
+            for o in range(outs):
+                last = o == outs - 1  # the cycle edge i -> i + 1
+                dst = ids[(i + 1) % n] if last else ids[rng.randrange(n)]
+                if bp and o == 0 and not last and rng.random() < 0.5:
+                    dst = bp
+                parts += ["<transition>", f'<source ref="{ids[i]}"/>', f'<target ref="{dst}"/>']
+                if rng.random() < 0.7:
+                    parts.append(_label("guard", guard(lints, dbls, clocks)))
+                if rng.random() < 0.2:
+                    parts.append(_label("synchronisation", "b" + rng.choice(["!", "?"])))
+                ups = [f"{rng.choice(ints + (['w'] if 'w' in lints else []) + dbls)} = "
+                       f"{expr(3, lints, dbls, cond_ok=True)}" for _ in range(rng.randint(0, 3))]
+                if clocks and rng.random() < 0.4:
+                    ups.append("x = 0")
+                if ups:
+                    parts.append(_label("assignment", ", ".join(ups)))
+                if rng.random() < 0.2:
+                    parts.append(_label("probability", str(rng.randint(1, 5))))
+                parts.append("</transition>")
+        if bp:
+            for _ in range(rng.randint(1, 3)):
+                parts += ["<transition>", f'<source ref="{bp}"/>', f'<target ref="{ids[rng.randrange(n)]}"/>',
+                          _label("probability", str(rng.randint(1, 5)))]
+                if rng.random() < 0.5:
+                    parts.append(_label("assignment", f"{rng.choice(ints)} = {expr(2, lints, dbls)}"))
+                parts.append("</transition>")
+        parts.append("</template>")
+        names.append(name)
+    parts += [f"<system>system {', '.join(names)};</system>", "</nta>"]
+    return Workload(f"zoo{'_full' if full else ''}_{seed}", "\n".join(parts) + "\n", var_id=0, threshold=3,
+                    horizon=50, runs=10_000)

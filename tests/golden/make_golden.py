@@ -55,10 +55,18 @@ FIXTURES = [
 ]
 
 
+# expression-zoo seeds whose models the reference front end accepts (the
+# reference-subset generator and the full one)
+ZOO_SEEDS = [0, 1, 2, 4, 5]
+ZOO_FULL_SEEDS = [60, 73]
+
+
 def generated():
     ws = [netgen.epidemic(), netgen.mutex(8), netgen.mutex(32)]
     ws += [netgen.random_network(s) for s in range(4)]
     ws += netgen.batch_networks(6)
+    ws += [netgen.expression_zoo(s) for s in ZOO_SEEDS]
+    ws += [netgen.expression_zoo(s, full=True) for s in ZOO_FULL_SEEDS]
     return ws
 
 

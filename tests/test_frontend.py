@@ -29,6 +29,11 @@ def _generated():
     ws = {w.name: w for w in [netgen.epidemic(), netgen.mutex(8), netgen.mutex(32)]}
     ws.update({w.name: w for w in [netgen.random_network(s) for s in range(4)]})
     ws.update({w.name: w for w in netgen.batch_networks(6)})
+    for m in MANIFEST["models"]:  # expression-zoo models: zoo_<seed>, zoo_full_<seed>
+        if m["generated"] and m["name"].startswith("zoo_"):
+            full = m["name"].startswith("zoo_full_")
+            w = netgen.expression_zoo(int(m["name"].rsplit("_", 1)[1]), full=full)
+            ws[w.name] = w
     return ws
 
 
@@ -83,3 +88,33 @@ def test_missing_file_is_a_model_error():
     with pytest.raises(api._native.CsmcError) as e:
         api.compile_model("/nonexistent/model.xml")
     assert e.value.code == api._native.CSMC_ERR_MODEL
+
+
+REFDUMP = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "refdump")
+
+
+@pytest.mark.skipif(not os.path.exists(REFDUMP), reason="the reference front-end dump tool is not built")
+@pytest.mark.parametrize("full", [False, True], ids=["reference-subset", "full"])
+def test_expression_zoo_matches_reference_front_end(tmp_path, full):
+    """Differential check against the reference's own parser, optimizer and
+    PN compiler (oracle/_ref/refdump) on 60 random expression-zoo models:
+    both accept with byte-identical networks, or both reject."""
+    import subprocess
+    from cusmc_b200 import _native
+    outcome = {"match": 0, "both_reject": 0}
+    for seed in range(60, 120) if full else range(60):
+        w = netgen.expression_zoo(seed, full=full)
+        path = w.write(str(tmp_path / f"{w.name}.xml"))
+        ref = subprocess.run([REFDUMP, path, "", "var"], capture_output=True, text=True, timeout=120)
+        try:
+            ours = api.dump_model(path, "", False)
+        except _native.CsmcError:
+            ours = None
+        if ref.returncode == 0:
+            assert ours is not None, f"seed {seed}: the reference accepts, this front end rejects"
+            assert ours == ref.stdout, f"seed {seed}: the networks differ"
+            outcome["match"] += 1
+        else:
+            assert ours is None, f"seed {seed}: the reference rejects, this front end accepts"
+            outcome["both_reject"] += 1
+    assert outcome["match"] > 0 and outcome["both_reject"] > 0, outcome
