@@ -246,10 +246,15 @@ def run_ours(args):
 
     # end to end through the host-buffer C-ABI call (rank-local)
     e2e_ms = []
+    e2e_kernel_ms = []
+    e2e_sampler = ClockSampler(local)
+    e2e_sampler.start()
     for s in range(args.steps):
         t0 = time.perf_counter()
-        api.run_host(blob, q, SEED, n, first_run_of(2000 + s))
+        r_host, _, _, _ = api.run_host(blob, q, SEED, n, first_run_of(2000 + s))
         e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+        e2e_kernel_ms.append(r_host.kernel_ms)
+    e2e_clocks = e2e_sampler.stop()
     e2e_t = sum(e2e_ms)
     if world > 1:
         t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
@@ -287,7 +292,8 @@ def run_ours(args):
         "race_steps_per_run": steps_total / runs_total,
         "component_steps_per_s": comp_steps / (t_total / 1000.0),
         "e2e": {"value": e2e_value, "unit": "runs/s", "h2d_bytes_per_step": len(blob),
-                "d2h_bytes_per_step": 9 * n},
+                "d2h_bytes_per_step": 9 * n, "ms_per_step": e2e_t / args.steps,
+                "kernel_ms_per_step": sum(e2e_kernel_ms) / args.steps, "clocks": e2e_clocks},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": None if traffic_per_run is None else traffic_per_run * n,
