@@ -491,6 +491,14 @@ def run_rare_is(args):
         if (p > 0 and half <= 0.1 * p) or n >= 10_000_000:
             break
     is_s = time.perf_counter() - t1
+    # optional fixed-size evaluation of the trained proposal (the survey's
+    # protocol: 1e7 weighted runs), outside the timed figure
+    evaluation = None
+    if args.is_eval_runs:
+        t_eval = time.perf_counter()
+        p_e, half_e, dev_e = P.estimate(net, q, prop, 19, args.is_eval_runs, first_run=3_000_000_000)
+        evaluation = {"runs": args.is_eval_runs, "estimate": p_e, "ci_half": half_e, "device_s": dev_e,
+                      "wall_s": time.perf_counter() - t_eval}
     # plain SMC: measured rate, and an estimate on a bounded sample
     plain_n = args.runs or 100_000_000
     hits = 0
@@ -515,7 +523,7 @@ def run_rare_is(args):
             "is": {"estimate": p, "ci_half": half, "runs": n, "train_s": train_s, "sample_s": is_s},
             "plain": {"estimate": p_plain, "ci_half": half_plain, "runs": plain_n, "runs_per_s": plain_rate,
                       "runs_for_10pct": need_plain, "seconds_for_10pct": plain_to_10},
-            "speedup": plain_to_10 / (train_s + is_s),
+            "speedup": plain_to_10 / (train_s + is_s), "is_evaluation": evaluation,
             "agree": abs(p - p_plain) <= half + half_plain,
             "ce_log": log.rounds}
     net.close()
@@ -624,6 +632,8 @@ def main():
     ap.add_argument("--runs", type=int, default=0,
                     help="runs per step per GPU (default: the workload's run count, 1e6 for the epidemic; "
                          "smaller values are for profiling captures)")
+    ap.add_argument("--is-eval-runs", type=int, default=0,
+                    help="rare_is: also evaluate the trained proposal on this many weighted runs (e.g. 10000000)")
     ap.add_argument("--batch-divisor", type=int, default=0,
                     help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
     ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "is_kernel", "mlp_grad"],
