@@ -52,11 +52,14 @@ def test_zero_tilt_is_the_plain_run():
     assert np.all(out["logw"] == 0.0)
 
 
-@pytest.mark.parametrize("which", ["epidemic", "random"])
+@pytest.mark.parametrize("which", ["epidemic", "epidemic_min", "random"])
 def test_weighted_estimate_is_unbiased(which):
     if which == "epidemic":
         w = netgen.epidemic(n_agents=20)
         q = api.variable_query(w.var_id, 40, threshold=9, is_max=True)
+    elif which == "epidemic_min":  # a min query: the susceptible count falls below 12
+        w = netgen.epidemic(n_agents=20)
+        q = api.variable_query(0, 40, threshold=12, is_max=False)
     else:
         w = netgen.random_network(3)
         q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
