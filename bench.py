@@ -20,8 +20,9 @@ cusmc_b200.netgen.epidemic; every step uses a fresh stretch of the random
 stream).  `value` is whole-job runs/s with the network already resident on
 the device, timed with CUDA events on the launching stream around the
 simulation kernels; `e2e` is the same metric through the host-buffer C-ABI
-call csmc_run_host (network upload, simulation, per-run flag/value copies
-back to pageable host memory, all inside the timed region).  Under torchrun
+call csmc_run_host (the network copied to the device, the simulation, the
+per-run flags and values copied back into host arrays, all inside the timed
+region, after as many untimed warm-up calls as the device-side measurement).  Under torchrun
 every rank simulates its own run range (weak scaling, no data-path
 collective); times are the max over ranks.
 
@@ -244,14 +245,20 @@ def run_ours(args):
     runs_total = n * args.steps * world
     value = runs_total / (t_total / 1000.0)
 
-    # end to end through the host-buffer C-ABI call (rank-local)
+    # end to end through the host-buffer C-ABI call (rank-local): every step
+    # copies the network to the device and the per-run flags and values back
+    # into the same host arrays (a caller's reused result buffers)
+    h_flags = np.empty(n, dtype=np.uint8)
+    h_values = np.empty(n, dtype=np.float64)
+    for s in range(args.warmup):
+        api.run_host(blob, q, SEED, n, first_run_of(3000 + s), out=(h_flags, h_values, None))
     e2e_ms = []
     e2e_kernel_ms = []
     e2e_sampler = ClockSampler(local)
     e2e_sampler.start()
     for s in range(args.steps):
         t0 = time.perf_counter()
-        r_host, _, _, _ = api.run_host(blob, q, SEED, n, first_run_of(2000 + s))
+        r_host, _, _, _ = api.run_host(blob, q, SEED, n, first_run_of(2000 + s), out=(h_flags, h_values, None))
         e2e_ms.append((time.perf_counter() - t0) * 1000.0)
         e2e_kernel_ms.append(r_host.kernel_ms)
     e2e_clocks = e2e_sampler.stop()
@@ -278,35 +285,39 @@ def run_ours(args):
     # 32 B of run state and network records in shared memory
     comp_steps = steps_total * n_comps  # all ranks
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    smem_peak = 128.0 * 148 * sm_mhz * 1e6 / 1e9  # GB/s: 128 B/clk/SM
+    smem_gbs, smem_mhz = api.measure_smem_bandwidth()
     smem_achieved = 32.0 * comp_steps / world / (t_kernel / 1000.0) / 1e9
     line = {
         "metric": metric_of(args.workload), "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 expressions", "data": "synthetic (seeded generated network)",
-        "config": {"workload": f"{args.workload} ({WORKLOADS[args.workload][1]}), {n} runs per step per GPU",
-                   "runs_per_step_per_gpu": n, "lanes_per_run": lanes, "comps_per_lane": cpl,
-                   "runs_per_cta": rpc, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"runs sharded over {world} GPU(s)"},
+        "config": bench_config(args.workload, n, world),
+        "plan": {"lanes_per_run": lanes, "comps_per_lane": cpl, "runs_per_cta": rpc},
         "estimate": hits / runs_total,
         "race_steps_per_run": steps_total / runs_total,
         "component_steps_per_s": comp_steps / (t_total / 1000.0),
         "e2e": {"value": e2e_value, "unit": "runs/s", "h2d_bytes_per_step": len(blob),
                 "d2h_bytes_per_step": 9 * n, "ms_per_step": e2e_t / args.steps,
                 "kernel_ms_per_step": sum(e2e_kernel_ms) / args.steps, "clocks": e2e_clocks},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
+        # the binding roofline: 32 B of shared-memory work per component-step
+        # over the shared-memory bandwidth measured on this GPU by a streaming
+        # 16-byte shared-load kernel (csmc_measure_smem_bandwidth)
+        "roofline": {"bound": "smem", "achieved": smem_achieved, "peak": smem_gbs, "unit": "GB/s",
+                     "frac": smem_achieved / smem_gbs,
                      "traffic": None if traffic_per_run is None else traffic_per_run * n,
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6650 GB/s",
-                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
-                     "note": "HBM is not what bounds this kernel (9 B per run of results); the binding "
-                             "resources are instruction issue and shared memory, below"},
-        "issue_roofline": {"bound": "shared memory / issue", "unit": "GB/s",
-                           "bytes_per_component_step": 32, "achieved": smem_achieved, "peak": smem_peak,
-                           "frac": smem_achieved / smem_peak,
-                           "peak_source": f"128 B/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (median SM clock sampled "
-                                          "during the timed steps)"},
+                     "peak_source": f"measured: streaming 16-byte shared-memory loads on every SM "
+                                    f"({smem_mhz:.0f} MHz sampled during that kernel)",
+                     "bytes_per_component_step": 32, "component_steps_per_launch": comp_steps / world / args.steps,
+                     "launch_ms": launch_ms,
+                     "traffic_note": "traffic = ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                     "(the kernel's HBM traffic: results only)"},
+        "hbm_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": None if traffic_per_run is None else traffic_per_run * n,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
+                         "note": "HBM does not bound this kernel (9 B of results per run)"},
         "clocks": clocks,
         "gpu_launches": 2 * args.steps,
         "wall_s": wall,
@@ -321,28 +332,67 @@ def run_ours(args):
         print(json.dumps(line))
 
 
+def _netgen_standalone():
+    """cusmc_b200/netgen.py loaded as a lone module: the reference arm uses it
+    to write the model file and nothing else of this package (no libcsmc)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("csmc_netgen_standalone",
+                                                  os.path.join(ROOT, "cusmc_b200", "netgen.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bench_config(name, n, world):
+    """The `config` both arms report for workload `name` at n runs per step
+    per GPU (identical keys and values, so the two lines describe one
+    workload)."""
+    return {"workload": f"{name} ({WORKLOADS[name][1]}), {n} runs per step per GPU",
+            "runs_per_step_per_gpu": n,
+            "l2": "cold between timed steps (our arm: 256 MB L2 flush; reference arm: a fresh process per step)",
+            "parallelism": f"runs sharded over {world} GPU(s)"}
+
+
+# reference arm: warm-up steps are untimed and each is a separate process,
+# so they run this many runs each (the timed steps run the full workload)
+REF_WARMUP_RUNS = 20_000
+
+
 def run_reference(args):
+    """The reference cuSMC binary (oracle/_ref/cusmc_ref_v*, built from the
+    reference sources for sm_100a with raised variable/edge limits) through
+    its stock CLI (main.cu:39-110 -> smc.cu:283-491 -> simulation_kernel,
+    smc.cu:237), on the same generated model file and query as our arm, at
+    the same runs per step.  Each step is one process; the step time is the
+    reference's own "Time taken" window (kernel + synchronise,
+    smc.cu:234-255).  Nothing of this package is loaded here except the
+    stand-alone network generator (no libcsmc)."""
     rank, world, _ = _env_rank()
     if rank != 0:
         return
-    from cusmc_b200 import api
-    w, path, blob, q = workload_blob(args.workload)
+    netgen = _netgen_standalone()
+    gens = {"epidemic_100": lambda: netgen.epidemic(n_agents=100, runs=RUNS_PER_STEP),
+            "random_0": lambda: netgen.random_network(0, runs=10_000),
+            "mutex_8": lambda: netgen.mutex(8), "mutex_32": lambda: netgen.mutex(32),
+            "mutex_64": lambda: netgen.mutex(64), "mutex_256": lambda: netgen.mutex(256)}
+    w = gens[args.workload]()
+    n = args.runs or w.runs
     # the smallest limits build that holds the network's variables
-    n_vars = api.blob_info(blob)["n_vars"]
-    variant = next((v for v in (8, 16, 64, 512) if v >= n_vars), None)
+    variant = next((v for v in (8, 16, 64, 512) if v >= w.n_vars), None)
     binary = os.path.join(ROOT, "oracle", "_ref", f"cusmc_ref_v{variant}")
     if variant is None or not os.path.exists(binary):
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/cusmc_ref_v{variant} was not built "
                           "(the reference checkout is needed at build time)"}))
         return
     work = tempfile.mkdtemp(prefix="csmc_ref_")
+    path = w.write(os.path.join(work, args.workload + ".xml"))
     cwd = os.path.join(work, "run")  # the reference writes ../results5.csv
     os.makedirs(cwd)
 
     def once(runs, seed):
         cmd = [binary, "-m", path, "-s", str(seed), "-q", str(runs), str(w.horizon), str(w.threshold),
                str(w.var_id), "1", "0", ""]
-        out = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
+        out = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=1500)
         ms = None
         result = None
         for line in out.stdout.splitlines():
@@ -354,29 +404,36 @@ def run_reference(args):
             raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
         return ms, result
 
-    probe_ms, _ = once(20_000, 1)
-    rate = 20_000 / (probe_ms / 1000.0)
-    sample = int(min(args.runs or w.runs, max(20_000, rate * 10.0)))
     for s in range(args.warmup):
-        once(sample, 100 + s)
+        once(min(n, REF_WARMUP_RUNS), 100 + s)
+    sampler = ClockSampler(0)
+    sampler.start()
     times, results = [], []
+    t_wall = time.perf_counter()
     for s in range(args.steps):
-        ms, res = once(sample, 1 + s)
+        ms, res = once(n, 1 + s)
         times.append(ms)
         results.append(res)
-    value = sample * args.steps / (sum(times) / 1000.0)
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    value = n * args.steps / (sum(times) / 1000.0)
     line = {
         "metric": metric_of(args.workload), "value": value, "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sum(times) / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 state / f64 expressions",
         "data": "synthetic (seeded generated network)", "impl": "reference",
-        "config": {"workload": f"{args.workload} ({WORKLOADS[args.workload][1]})",
-                   "runs_per_step": sample, "binary": f"reference cuSMC built for sm_100a, MAX_VARIABLES={variant}, "
-                                                     "MAX_EDGES_PER_NODE=8"},
+        "config": bench_config(args.workload, n, 1),
+        "binary": f"reference cuSMC built from its sources for sm_100a, MAX_VARIABLES={variant}, "
+                  "MAX_EDGES_PER_NODE=8 (oracle/ref/Makefile)",
+        "warmup_runs_per_step": min(n, REF_WARMUP_RUNS),
         "estimate": statistics.mean(results) if results else None,
+        "clocks": clocks, "wall_s": wall,
+        # the reference's simulation path is a GPU kernel: it has no CPU
+        # implementation, so this describes a GPU run of the reference
         "cpu_baseline": {"value": value, "unit": "runs/s", "cores": 1, "kind": "reference",
-                         "sample": f"{sample} runs per step; the reference's simulation path is its GPU kernel "
-                                   "(it has no CPU implementation)"},
+                         "where": "GPU (B200): the reference has no CPU implementation of the simulation; "
+                                  "one host thread drives its kernel",
+                         "sample": f"{n} runs per step, {args.steps} steps, one reference process per step"},
         "e2e": {"value": value, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -24,6 +24,17 @@ CSMC_ERR_TIMEOUT = -6
 QUERY_LOCATION = 0
 QUERY_VARIABLE = 1
 
+# csmc_numeric_eval function codes (include/csmc.h)
+NUM_PHILOX = 0
+NUM_EXP_DELAY = 1
+NUM_LOG2_F32 = 2
+NUM_LOG2_F64 = 3
+NUM_EXP2_F64 = 4
+NUM_POW_F64 = 5
+NUM_EXP2_F32 = 6
+NUM_GELU_F32 = 7
+NUM_GELU_GRAD_F32 = 8
+
 
 class Query(ctypes.Structure):
     """csmc_query."""
@@ -88,6 +99,7 @@ _SIGNATURES = {
     "csmc_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(Query), ctypes.c_uint64,
                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.POINTER(Result)]),
+    "csmc_run_host_release": (None, []),
     "csmc_run_verify": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_uint64, ctypes.c_uint64,
                                        ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),
@@ -135,6 +147,9 @@ _SIGNATURES = {
                                         ctypes.c_void_p]),
     "csmc_mlp_grad": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "csmc_numeric_eval": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "csmc_measure_smem_bandwidth": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 }
 
 

@@ -244,12 +244,21 @@ class Batch:
         return out
 
 
-def run_host(blob: bytes, query: Query, seed: int, n_runs: int, first_run: int = 0, want_steps: bool = False):
+def run_host(blob: bytes, query: Query, seed: int, n_runs: int, first_run: int = 0, want_steps: bool = False,
+             out: tuple | None = None):
     """Host buffers in and out (upload, kernel, copies back). Returns
-    (Result, flags, values, steps-or-None) with numpy arrays."""
-    flags = np.zeros(n_runs, dtype=np.uint8)
-    values = np.zeros(n_runs, dtype=np.float64)
-    steps = np.zeros(n_runs, dtype=np.uint32) if want_steps else None
+    (Result, flags, values, steps-or-None) with numpy arrays.  out: optional
+    (flags uint8, values float64, steps uint32 or None) arrays of at least
+    n_runs entries to fill instead of new ones."""
+    if out is not None:
+        flags, values, steps = out
+        for a, dt in ((flags, np.uint8), (values, np.float64), (steps, np.uint32)):
+            if a is not None and (a.dtype != dt or a.size < n_runs or not a.flags.c_contiguous):
+                raise ValueError("run_host: output arrays must be contiguous, of the right type and size")
+    else:
+        flags = np.empty(n_runs, dtype=np.uint8)
+        values = np.empty(n_runs, dtype=np.float64)
+        steps = np.empty(n_runs, dtype=np.uint32) if want_steps else None
     r = Result()
     check(lib().csmc_run_host(blob, len(blob), ctypes.byref(query), seed & (2**64 - 1), first_run, n_runs,
                               flags.ctypes.data, values.ctypes.data,
@@ -283,12 +292,20 @@ def smc_ex(model: str, seed: int, sims: int, query: Query, loc_query: str = "", 
                             json_path.encode() if json_path else None, runs_path.encode() if runs_path else None))
 
 
+def measure_smem_bandwidth() -> tuple[float, float]:
+    """Measured shared-memory bandwidth of the current device: (GB/s, mean
+    SM clock in MHz during the measurement)."""
+    gbs, mhz = ctypes.c_double(), ctypes.c_double()
+    check(lib().csmc_measure_smem_bandwidth(ctypes.byref(gbs), ctypes.byref(mhz)))
+    return gbs.value, mhz.value
+
+
 def version() -> str:
     return lib().csmc_version().decode()
 
 
 __all__ = [
     "Batch", "Configuration", "StatisticsConfiguration", "Network", "Query", "Result", "compile_model", "dump_model",
-    "blob_info", "make_query", "parse_query", "smc_ex", "location_query", "variable_query", "run_host", "smc", "version",
+    "blob_info", "make_query", "measure_smem_bandwidth", "parse_query", "smc_ex", "location_query", "variable_query", "run_host", "smc", "version",
     "QUERY_LOCATION", "QUERY_VARIABLE", "_native",
 ]

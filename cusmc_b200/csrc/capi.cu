@@ -512,51 +512,6 @@ int csmc_run_verify(const csmc_net *net, const csmc_query *q, uint64_t seed, uin
     }
 }
 
-int csmc_run_host(const void *blob, size_t bytes, const csmc_query *q, uint64_t seed, uint64_t first_run,
-                  uint64_t n_runs, uint8_t *flags, double *values, uint32_t *steps, csmc_result *out) {
-    csmc_net *n = nullptr;
-    int rc = csmc_net_upload(blob, bytes, &n);
-    if (rc) return rc;
-    uint8_t *d_flags = nullptr;
-    double *d_values = nullptr;
-    uint32_t *d_steps = nullptr;
-    auto cleanup = [&] {
-        cudaFree(d_flags);
-        cudaFree(d_values);
-        cudaFree(d_steps);
-        csmc_net_free(n);
-    };
-    if (n_runs) {
-        if (cudaMalloc(&d_flags, n_runs) != cudaSuccess || cudaMalloc(&d_values, n_runs * sizeof(double)) != cudaSuccess ||
-            (steps && cudaMalloc(&d_steps, n_runs * sizeof(uint32_t)) != cudaSuccess)) {
-            cleanup();
-            return fail(CSMC_ERR_CUDA, "cudaMalloc(per-run outputs)");
-        }
-    }
-    rc = csmc_run(n, q, seed, first_run, n_runs, d_flags, d_values, d_steps, out, nullptr);
-    if (rc == CSMC_OK && n_runs) {
-        std::vector<double> v(values ? 0 : n_runs);
-        double *hv = values ? values : v.data();
-        cudaError_t e = cudaMemcpy(hv, d_values, n_runs * sizeof(double), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess && flags) e = cudaMemcpy(flags, d_flags, n_runs, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess && steps) e = cudaMemcpy(steps, d_steps, n_runs * sizeof(uint32_t), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(per-run outputs)");
-        else {
-            // the reference's host reduction order (smc.cu:378-402)
-            double s = 0.0, s2 = 0.0;
-            for (uint64_t i = 0; i < n_runs; ++i) {
-                s += hv[i];
-                s2 += hv[i] * hv[i];
-            }
-            out->sum = s;
-            out->sum_sq = s2;
-            if (q->kind == CSMC_QUERY_VARIABLE && q->is_estimate) out->estimate = s / static_cast<double>(n_runs);
-        }
-    }
-    cleanup();
-    return rc;
-}
-
 }  // extern "C"
 
 namespace {

@@ -134,6 +134,12 @@ int main(int argc, char *argv[]) {
                 return 0;
             }
             loc = buf;
+            if (n > static_cast<uint64_t>(INT32_MAX)) {
+                // the report and the timing CSV carry the run count as int
+                // (the reference's statistics_Configuration::simulations)
+                std::cerr << "Error: the formula's run count " << n << " exceeds " << INT32_MAX << std::endl;
+                return 0;
+            }
             if (n) sims = static_cast<int>(n);
         } else {
             q.kind = st.var_id == -1 ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;

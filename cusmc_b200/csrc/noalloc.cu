@@ -15,8 +15,10 @@
 #include "../../include/csmc.h"
 #include "include/csmc_net.h"
 #include "include/csmc_numeric.h"
+#include "kernels/reduce.cuh"
 #include "kernels/sim.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -33,19 +35,12 @@ namespace {
 // bytes per device.  Layout: [0, 64) counters, [64, 64 + 4096) partial sums,
 // [kSlabOffset, end) run-state slabs of the thread-per-run kernel.
 constexpr size_t kScratchBytes = CSMC_NOALLOC_SCRATCH_BYTES;
-constexpr int kReduceBlocks = 256;
+using csmc::kReduceBlocks;
 constexpr size_t kPartialOffset = 64;
 constexpr size_t kSlabOffset = 8192;
 static_assert(kPartialOffset + 2 * kReduceBlocks * sizeof(double) <= kSlabOffset, "scratch layout");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-// Device address of g_noalloc_scratch per device ordinal, looked up once per
-// device with that device current.  In host code the symbol itself is only a
-// host-side stand-in, never a device address.
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void *g_scratch_ptr[kMaxDevices] = {};
 
 int fail(int code, const std::string &m) {
     csmc::set_last_error(m);  // reported by csmc_last_error()
@@ -56,49 +51,75 @@ int cuda_fail(cudaError_t e, const char *what) {
     return fail(CSMC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// The current context's unique id (cuCtxGetId), through driver entry points
+// fetched from the runtime, so the library does not link the driver itself.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+int current_context_id(int dev, unsigned long long *id) {
+    static std::once_flag once;
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(b);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return fail(CSMC_ERR_CUDA, "driver entry points cuCtxGetCurrent/cuCtxGetId");
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) {
+        // no context current on this thread yet: make the device's primary
+        // context current (cudaSetDevice initialises it)
+        const cudaError_t e = cudaSetDevice(dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+        if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return fail(CSMC_ERR_CUDA, "no current CUDA context");
+    }
+    if (get_id(ctx, id) != CUDA_SUCCESS) return fail(CSMC_ERR_CUDA, "cuCtxGetId");
+    return CSMC_OK;
+}
+
+// Device address of g_noalloc_scratch per device ordinal, looked up with
+// that device current and kept together with the id of the context it was
+// looked up in: a call from another context on the same device (after a
+// cudaDeviceReset, or from a non-primary context) looks the address up
+// again instead of using a stale one.  In host code the symbol itself is
+// only a host-side stand-in, never a device address.
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+void *g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
 int scratch_for_current_device(void **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return fail(CSMC_ERR_LIMIT, "device ordinal out of range");
+    unsigned long long ctx = 0;
+    int rc = current_context_id(dev, &ctx);
+    if (rc) return rc;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
         g_scratch_ptr[dev] = p;
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_ptr[dev];
     return CSMC_OK;
 }
 
 // Deterministic sum and sum of squares of values[0..n) into partials[2*b],
-// partials[2*b+1] per block b: fixed chunking, fixed per-thread order and a
-// fixed shared-memory tree (the same arithmetic as csmc_run's reduction).
+// partials[2*b+1] per block b: csmc_run's reduction (kernels/reduce.cuh),
+// so the sums carry the same bits as csmc_run's.
 __global__ void noalloc_reduce(const double *values, uint64_t n, double *partials) {
-    __shared__ double s1[256], s2[256];
-    const uint64_t chunk = (n + kReduceBlocks - 1) / kReduceBlocks;
-    const uint64_t b0 = blockIdx.x * chunk, b1 = (b0 + chunk < n) ? b0 + chunk : n;
-    double a = 0.0, q = 0.0;
-    for (uint64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        const double v = values[i];
-        a = csmc::d_add(a, v);
-        q = csmc::d_add(q, csmc::d_mul(v, v));
-    }
-    s1[threadIdx.x] = a;
-    s2[threadIdx.x] = q;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            s1[threadIdx.x] = csmc::d_add(s1[threadIdx.x], s1[threadIdx.x + s]);
-            s2[threadIdx.x] = csmc::d_add(s2[threadIdx.x], s2[threadIdx.x + s]);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = s1[0];
-        partials[2 * blockIdx.x + 1] = s2[0];
-    }
+    csmc::reduce_block(values, n, blockIdx.x, partials + 2 * blockIdx.x);
 }
 
 }  // namespace

@@ -39,6 +39,8 @@ class Workload:
     loc_query: str = ""
     is_max: bool = True
     is_estimate: bool = False
+    n_vars: int = 0      # int and clock variables the network declares (what the
+                         # reference's variable registry counts; 0: not recorded)
 
     def cli_query(self) -> list[str]:
         """The reference CLI's -q arguments for this workload."""
@@ -124,7 +126,7 @@ def epidemic(n_agents: int = 100, beta: float = 0.3, rate_ei: float = 0.2, rate_
         trans += [(i, r, [("assignment", "I = I - 1, R = R + 1")])]
         d.template(f"Agent{k}", "", locs, i if k == 0 else s, trans)
     return Workload(f"epidemic_{n_agents}", d.finish(), var_id=3, threshold=r_threshold - 1, horizon=horizon,
-                    runs=runs)
+                    runs=runs, n_vars=4)
 
 
 def mutex(n: int = 32, k: int = 2, horizon: int = 200, runs: int = 10_000_000) -> Workload:
@@ -148,7 +150,7 @@ def mutex(n: int = 32, k: int = 2, horizon: int = 200, runs: int = 10_000_000) -
             (cs, idle, [("assignment", "id = 0, incs = incs - 1")]),
         ]
         d.template(f"P{p}", f"clock x;\nconst int pid = {p + 1};", locs, idle, trans)
-    return Workload(f"mutex_{n}", d.finish(), var_id=1, threshold=1, horizon=horizon, runs=runs)
+    return Workload(f"mutex_{n}", d.finish(), var_id=1, threshold=1, horizon=horizon, runs=runs, n_vars=2 + n)
 
 
 def random_network(seed: int, n_comps: int = 8, n_locs: int = 4, n_edges: int = 6, horizon: int = 100,
@@ -218,7 +220,8 @@ def random_network(seed: int, n_comps: int = 8, n_locs: int = 4, n_edges: int = 
             trans.extend(e[1] for e in lst)
         init = ids[rng.randrange(n_locs)]
         d.template(f"C{c}", "clock x;", locs, init, trans)
-    return Workload(f"random_{seed}", d.finish(), var_id=0, threshold=target - 1, horizon=horizon, runs=runs)
+    return Workload(f"random_{seed}", d.finish(), var_id=0, threshold=target - 1, horizon=horizon, runs=runs,
+                    n_vars=2 + n_comps)
 
 
 def batch_networks(count: int = 64, base_seed: int = 1000):

@@ -110,10 +110,20 @@ void csmc_net_free(csmc_net *net);
 int csmc_run(const csmc_net *net, const csmc_query *q, uint64_t seed, uint64_t first_run, uint64_t n_runs,
              uint8_t *flags, double *values, uint32_t *steps, csmc_result *out, void *stream);
 
-/* As csmc_run, from a host blob to host outputs (upload, run, copy back;
- * all copies included).  Host output pointers may be NULL. */
+/* As csmc_run, from a host blob to host outputs: the blob is copied to the
+ * device, the runs simulated, and the per-run outputs copied back into the
+ * host buffers (any may be NULL) on every call.  out->sum and out->sum_sq
+ * are summed on the host in run order (the reference's host reduction).
+ * The library keeps, per device, the network handle of the last blob (its
+ * launch plan is reused while the bytes stay the same), device output
+ * buffers, pinned staging buffers and a stream; calls on one device are
+ * serialised. */
 int csmc_run_host(const void *blob, size_t bytes, const csmc_query *q, uint64_t seed, uint64_t first_run,
                   uint64_t n_runs, uint8_t *flags, double *values, uint32_t *steps, csmc_result *out);
+
+/* Frees what csmc_run_host keeps per device (no counterpart in the
+ * reference). */
+void csmc_run_host_release(void);
 
 /* Verification variant: also returns, per run, a 64-bit digest of the event
  * sequence (winner, delay bits, chosen edge, update values, receivers) and the
@@ -280,6 +290,44 @@ int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, floa
 int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
                   void *stream);
 
+/* ---- Numeric primitives ----------------------------------------------------
+ * No counterpart in the reference, whose random stream is curand XORWOW
+ * (simulation/simulation.cu:756-760) and whose logarithm is the hardware
+ * __log2f (simulation.cu:529).  These are the functions whose exact bits
+ * define a run here; csmc_numeric_eval evaluates the device code of one of
+ * them over n elements of DEVICE arrays a (and b), writing out, and
+ * synchronises the stream.  Codes and operands:
+ *   CSMC_NUM_PHILOX        a: u32 counters[4n], b: u32 keys[2n] -> u32[4n]
+ *                          (Philox4x32-10, Salmon et al., SC'11)
+ *   CSMC_NUM_EXP_DELAY     a: u32 draws[n], b: f32 1/rate[n] -> f32 delay
+ *                          (-log2(u) / rate, u = ((x >> 8) + 1) 2^-24)
+ *   CSMC_NUM_LOG2_F32      a: f32[n] positive normal -> f32 log2
+ *   CSMC_NUM_LOG2_F64      a: f64[n] -> f64 log2
+ *   CSMC_NUM_EXP2_F64      a: f64[n] -> f64 2^a
+ *   CSMC_NUM_POW_F64       a, b: f64[n] -> f64 a^b (the model language's '^')
+ *   CSMC_NUM_EXP2_F32      a: f32[n] -> f32 2^a (proposal network)
+ *   CSMC_NUM_GELU_F32      a: f32[n] -> f32 GELU (tanh form)
+ *   CSMC_NUM_GELU_GRAD_F32 a: f32[n] -> f32 GELU' */
+#define CSMC_NUM_PHILOX 0
+#define CSMC_NUM_EXP_DELAY 1
+#define CSMC_NUM_LOG2_F32 2
+#define CSMC_NUM_LOG2_F64 3
+#define CSMC_NUM_EXP2_F64 4
+#define CSMC_NUM_POW_F64 5
+#define CSMC_NUM_EXP2_F32 6
+#define CSMC_NUM_GELU_F32 7
+#define CSMC_NUM_GELU_GRAD_F32 8
+int csmc_numeric_eval(int32_t fn, const void *a, const void *b, uint64_t n, void *out, void *stream);
+
+/* Measures the shared-memory bandwidth of the current device (no
+ * counterpart in the reference): a kernel on every SM streams conflict-free
+ * 16-byte shared-memory loads (about 5 GB per launch, best of three timed
+ * launches after one warm-up).  *gbs receives GB/s over the whole device;
+ * *sm_mhz (may be NULL) the mean SM clock during the timed launches, from
+ * clock64() against %globaltimer.  This is the peak the shared-memory
+ * roofline of the thread-per-run simulation kernel is quoted against. */
+int csmc_measure_smem_bandwidth(double *gbs, double *sm_mhz);
+
 /* Scratch bytes per device behind csmc_run_noalloc (held from the first
  * call on a device until the process exits). */
 #define CSMC_NOALLOC_SCRATCH_BYTES (2u * 1024u * 1024u)
@@ -302,8 +350,10 @@ int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *
  * CSMC_ERR_LIMIT; fewer CTAs are launched when the slabs would not all fit.
  *
  * The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Every call on a device shares the one array
+ * (cudaGetSymbolAddress) with that device current, and keeps it with the id
+ * of the current context; a later call from another context on that device
+ * (after cudaDeviceReset, or from a non-primary context) looks it up again.
+ * Make the first call in a context before any stream capture.  Every call on a device shares the one array
  * and overwrites what the previous call left there (the counters are cleared
  * at the start of each call): calls whose work overlaps on the GPU, from
  * several host threads or on several streams, race and return wrong counts.

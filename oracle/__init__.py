@@ -51,6 +51,9 @@ def lib():
         h.oracle_mlp_grad.restype = ctypes.c_int
         h.oracle_mlp_grad.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                       ctypes.POINTER(ctypes.c_double)]
+        h.oracle_numeric_eval.restype = ctypes.c_int
+        h.oracle_numeric_eval.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.c_void_p]
         _lib = h
     return _lib
 
@@ -132,3 +135,22 @@ def mlp_grad(params: bytes, rows: np.ndarray):
     if rc != 0:
         raise RuntimeError("oracle: " + lib().oracle_last_error().decode())
     return g, J.value
+
+
+# ---- numeric primitives -----------------------------------------------------
+
+_NUM_OUT = {0: np.uint32, 1: np.float32, 2: np.float32, 3: np.float64, 4: np.float64, 5: np.float64,
+            6: np.float32, 7: np.float32, 8: np.float32}
+
+
+def numeric(fn: int, a, b=None) -> np.ndarray:
+    """Host evaluation of a numeric primitive (csmc_numeric_eval's codes):
+    Philox takes counters (n, 4) and keys (n, 2) as uint32 and returns (n, 4)."""
+    a = np.ascontiguousarray(a)
+    b = None if b is None else np.ascontiguousarray(b)
+    n = a.shape[0]
+    out = np.zeros((n, 4) if fn == 0 else n, dtype=_NUM_OUT[fn])
+    rc = lib().oracle_numeric_eval(fn, a.ctypes.data, None if b is None else b.ctypes.data, n, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("oracle: " + lib().oracle_last_error().decode())
+    return out

@@ -456,6 +456,56 @@ extern "C" {
 
 const char *oracle_last_error(void) { return g_err.c_str(); }
 
+/* The numeric primitives on the host, over host arrays: the same function
+ * codes and operand layouts as csmc_numeric_eval (include/csmc.h). */
+int oracle_numeric_eval(int32_t fn, const void *a, const void *b, uint64_t n, void *out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        switch (fn) {
+        case CSMC_NUM_PHILOX: {
+            const uint32_t *c = static_cast<const uint32_t *>(a) + 4 * i;
+            const uint32_t *k = static_cast<const uint32_t *>(b) + 2 * i;
+            const csmc::u32x4 r = csmc::philox4x32_10(csmc::u32x4{c[0], c[1], c[2], c[3]}, k[0], k[1]);
+            uint32_t *o = static_cast<uint32_t *>(out) + 4 * i;
+            o[0] = r.x;
+            o[1] = r.y;
+            o[2] = r.z;
+            o[3] = r.w;
+            break;
+        }
+        case CSMC_NUM_EXP_DELAY:
+            static_cast<float *>(out)[i] =
+                csmc::exp_delay(static_cast<const uint32_t *>(a)[i], static_cast<const float *>(b)[i]);
+            break;
+        case CSMC_NUM_LOG2_F32:
+            static_cast<float *>(out)[i] = csmc::log2_pos(static_cast<const float *>(a)[i]);
+            break;
+        case CSMC_NUM_LOG2_F64:
+            static_cast<double *>(out)[i] = csmc::log2_d(static_cast<const double *>(a)[i]);
+            break;
+        case CSMC_NUM_EXP2_F64:
+            static_cast<double *>(out)[i] = csmc::exp2_d(static_cast<const double *>(a)[i]);
+            break;
+        case CSMC_NUM_POW_F64:
+            static_cast<double *>(out)[i] =
+                csmc::pow_model(static_cast<const double *>(a)[i], static_cast<const double *>(b)[i]);
+            break;
+        case CSMC_NUM_EXP2_F32:
+            static_cast<float *>(out)[i] = csmc::exp2_f(static_cast<const float *>(a)[i]);
+            break;
+        case CSMC_NUM_GELU_F32:
+            static_cast<float *>(out)[i] = csmc::gelu_f(static_cast<const float *>(a)[i]);
+            break;
+        case CSMC_NUM_GELU_GRAD_F32:
+            static_cast<float *>(out)[i] = csmc::gelu_grad_f(static_cast<const float *>(a)[i]);
+            break;
+        default:
+            g_err = "unknown numeric function";
+            return -1;
+        }
+    }
+    return 0;
+}
+
 /* Simulates runs with the reference semantics on `threads` host threads
  * (<= 0: all hardware threads).  Per-run outputs (host, may be NULL): flags,
  * values, steps, digests, final_state (n_comps + n_vars words per run).

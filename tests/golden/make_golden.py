@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures under tests/golden/ (run from the repo root
 in the build container, where the reference checkout and its build exist):
 
-  python tests/golden/make_golden.py [--ref /root/reference]
+  python tests/golden/make_golden.py [--ref REFERENCE_CHECKOUT]   (default: $CSMC_REFERENCE)
 
 * frontend/<model>.<mode>.dump — the network as the REFERENCE front end
   delivers it to its kernel (oracle/_ref/refdump: reference parser, optimizer,
@@ -72,7 +72,7 @@ def generated():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CSMC_REFERENCE", "/root/reference"))
     args = ap.parse_args()
     refdump = os.path.join(ROOT, "oracle", "_ref", "refdump")
     if not os.path.exists(refdump):

@@ -14,7 +14,8 @@ import pytest
 from conftest import GOLDEN
 from cusmc_b200 import api, netgen
 
-REF_XML = "/root/reference/xml_files"
+# the reference checkout (read-only); CSMC_REFERENCE overrides the default location
+REF_XML = os.path.join(os.environ.get("CSMC_REFERENCE", "/root/reference"), "xml_files")
 
 with open(os.path.join(GOLDEN, "manifest.json")) as f:
     MANIFEST = json.load(f)

@@ -10,7 +10,8 @@ import pytest
 
 from cusmc_b200 import api, netgen
 
-REF_XML = "/root/reference/xml_files"
+# the reference checkout (read-only); CSMC_REFERENCE overrides the default location
+REF_XML = os.path.join(os.environ.get("CSMC_REFERENCE", "/root/reference"), "xml_files")
 
 
 def _q(path, formula):
