@@ -339,6 +339,7 @@ def _netgen_standalone():
     spec = importlib.util.spec_from_file_location("csmc_netgen_standalone",
                                                   os.path.join(ROOT, "cusmc_b200", "netgen.py"))
     mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look their module up by name
     spec.loader.exec_module(mod)
     return mod
 

@@ -34,6 +34,7 @@ NUM_POW_F64 = 5
 NUM_EXP2_F32 = 6
 NUM_GELU_F32 = 7
 NUM_GELU_GRAD_F32 = 8
+NUM_PHILOX_STEP = 9
 
 
 class Query(ctypes.Structure):
@@ -70,6 +71,47 @@ class Result(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class CeConfig(ctypes.Structure):
+    """csmc_ce_config."""
+
+    _fields_ = [
+        ("rounds", ctypes.c_int32),
+        ("adam_steps", ctypes.c_int32),
+        ("runs_per_round", ctypes.c_uint64),
+        ("max_rows", ctypes.c_uint64),
+        ("rho", ctypes.c_double),
+        ("lr", ctypes.c_double),
+        ("settle", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+
+class CeRound(ctypes.Structure):
+    """csmc_ce_round."""
+
+    _fields_ = [
+        ("round", ctypes.c_int32),
+        ("elite", ctypes.c_int32),
+        ("rows", ctypes.c_uint64),
+        ("level", ctypes.c_double),
+        ("j_start", ctypes.c_double),
+        ("j_end", ctypes.c_double),
+        ("estimate", ctypes.c_double),
+        ("hits", ctypes.c_uint64),
+        ("capped", ctypes.c_uint64),
+        ("mean_steps", ctypes.c_double),
+        ("kernel_ms", ctypes.c_double),
+        ("run_s", ctypes.c_double),
+        ("trace_s", ctypes.c_double),
+        ("adam_s", ctypes.c_double),
+        ("at_goal", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
 
 
 class CsmcError(RuntimeError):
@@ -147,6 +189,18 @@ _SIGNATURES = {
                                         ctypes.c_void_p]),
     "csmc_mlp_grad": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "csmc_ce_select": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                      ctypes.c_double, ctypes.c_int32, ctypes.c_double, ctypes.c_uint64,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]),
+    "csmc_smc_is": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Query),
+                                   ctypes.POINTER(CeConfig), ctypes.c_char_p]),
+    "csmc_mlp_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "csmc_mlp_init": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_void_p]),
+    "csmc_is_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_uint64, ctypes.POINTER(CeConfig),
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(CeRound),
+                                     ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "csmc_numeric_eval": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                          ctypes.c_void_p, ctypes.c_void_p]),
     "csmc_measure_smem_bandwidth": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),

@@ -98,6 +98,25 @@ bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std:
         why = "thread-per-run plans use 32..128 threads per CTA";
         return false;
     }
+    if (family == 4) {  // class-coded thread per run (sim_coded.cuh)
+        if (!n->classes || h.n_comps > 256 || h.max_locs_per_comp > 32) {
+            why = "the class-coded plan needs race classes, at most 256 components and 32 locations per automaton";
+            return false;
+        }
+        const size_t slab = csmc::coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, n->slots, block);
+        if (n->bytes + slab > max_smem) {
+            why = "network and run state do not fit in shared memory";
+            return false;
+        }
+        n->family = 4;
+        n->lanes = 1;
+        n->comps_per_lane = static_cast<int>(h.n_comps);
+        n->block = block;
+        n->state_stride = static_cast<uint32_t>(slab);
+        n->state_in_global = false;
+        n->smem = n->bytes + slab;
+        return true;
+    }
     if (family == 2) {  // network and run state in global memory
         if (h.max_locs_per_comp > 0xffffu || h.n_locs > 0xffffu) {
             why = "more than 65535 locations";
@@ -210,8 +229,10 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     p.final_state = final_state;
     p.scratch = n->d_scratch;
     int ctas = 0;
+    p.keys = csmc::philox_keys(seed);
     int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
              : n->family == 2 ? csmc::batch_max_active_ctas(verify, n->block, n->smem, &ctas)
+             : n->family == 4 ? csmc::coded_max_active_ctas(verify, n->slots, n->block, n->smem, &ctas)
                               : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->classes,
                                                              n->block, n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
@@ -224,7 +245,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     if (grid > needed) grid = needed;
     n->grid = static_cast<int>(grid);
     p.state_global = nullptr;
-    if (n->family >= 1 && n->state_in_global) {
+    if ((n->family == 1 || n->family == 2) && n->state_in_global) {
         const size_t need = grid * static_cast<size_t>(n->state_stride);
         if (need > n->state_bytes) {
             cudaFree(n->d_state);
@@ -273,6 +294,7 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     rc = n->family == 0   ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block,
                                              n->smem, st)
          : n->family == 2 ? csmc::batch_launch(verify, bp, static_cast<int>(grid), n->block, st)
+         : n->family == 4 ? csmc::coded_launch(verify, n->slots, p, static_cast<int>(grid), n->block, n->smem, st)
                           : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, n->classes, p,
                                                 static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
@@ -425,15 +447,17 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     n->slots = h->max_edges_per_loc >= 2;
     n->loc8 = h->max_locs_per_comp <= 256;
     n->classes = (h->flags & CSMC_NET_RACE_CLASSES) != 0 && h->n_comps <= 256;
-    // default plan: one thread per run when the run state of a 128-thread
-    // CTA fits next to the network in shared memory, lane groups otherwise
+    // default plan: the class-coded thread-per-run kernel when the network
+    // has race classes and fits its limits; else one thread per run when the
+    // run state of a 128-thread CTA fits next to the network in shared
+    // memory, lane groups otherwise
     std::string why;
     int G = 0, K = 0;
     choose_shape(h->n_comps, G, K);
     const size_t per_thread = csmc::serial_state_bytes_per_thread(h->n_comps, h->n_vars, h->n_rate_prog, n->slots, n->loc8);
     const bool serial_fits = n->bytes + 128 * per_thread <= static_cast<size_t>(max_smem_optin(n->device));
-    bool ok = false;
-    if (serial_fits) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
+    bool ok = configure_plan(n.get(), 4, 1, static_cast<int>(h->n_comps), 128, why);
+    if (!ok && serial_fits) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
     if (!ok) ok = configure_plan(n.get(), 0, G, K, 256, why);
     if (!ok) ok = configure_plan(n.get(), 1, 1, static_cast<int>(h->n_comps), 128, why);
     if (!ok) ok = configure_plan(n.get(), 2, 1, static_cast<int>(h->n_comps), 128, why);

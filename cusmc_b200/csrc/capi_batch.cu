@@ -489,6 +489,7 @@ int csmc_autotune(csmc_net *n, const csmc_query *q, uint64_t seed, uint64_t prob
         K = 2;
         while (G * K < C) K <<= 1;
     }
+    for (int block : {64, 128}) cands.push_back({4, 1, C, block});
     for (int block : {64, 128}) cands.push_back({1, 1, C, block});
     for (int block : {128, 256}) cands.push_back({0, G, K, block});
     for (int block : {64, 128}) cands.push_back({2, 1, C, block});

@@ -13,8 +13,15 @@
 //                          -q fields except SIMS, which the formula's N overrides
 //   --csmc-json PATH       JSON summary (estimate, 95% CI, Chernoff-Hoeffding eps)
 //   --csmc-runs-csv PATH   every run's flag and tracked value
+//   --csmc-is              learned importance sampling for a variable
+//                          probability query: CE training of the proposal on
+//                          the GPU, then SIMS weighted runs (csmc_smc_is)
+//   --csmc-is-ce R,N,S,LR  its CE configuration: at most R rounds of N runs,
+//                          S Adam steps per round at step size LR
+//                          (default 12,10000,40,0.03)
 #include "../../../include/csmc.h"
 
+#include <cstdio>
 #include <iostream>
 #include <stdexcept>
 #include <string>
@@ -23,7 +30,24 @@ namespace {
 
 struct Extras {  // the --csmc- options
     std::string formula, json, runs_csv;
+    bool is = false;
+    csmc_ce_config ce{12, 40, 10000, 1000000, 0.1, 0.03, 1, 0};
 };
+
+bool parse_ce(const std::string &v, csmc_ce_config *ce) {
+    int r = 0, st = 0;
+    unsigned long long n = 0;
+    double lr = 0.0;
+    char tail = 0;
+    if (std::sscanf(v.c_str(), "%d,%llu,%d,%lf%c", &r, &n, &st, &lr, &tail) != 4 || r < 1 || n < 1 || st < 1 ||
+        !(lr > 0.0))
+        return false;
+    ce->rounds = r;
+    ce->runs_per_round = n;
+    ce->adam_steps = st;
+    ce->lr = lr;
+    return true;
+}
 
 struct StatConfig {  // statistics_Configuration, main.cuh:46-58
     int simulations = 16384;
@@ -38,7 +62,15 @@ struct StatConfig {  // statistics_Configuration, main.cuh:46-58
 bool handle_args(int argc, char **argv, std::string *filename, int *seed, StatConfig *stats, Extras *ex) {
     for (int i = 1; i < argc; i++) {
         std::string arg = argv[i];
-        if (arg == "--csmc-formula" || arg == "--csmc-json" || arg == "--csmc-runs-csv") {
+        if (arg == "--csmc-is") {
+            ex->is = true;
+        } else if (arg == "--csmc-is-ce") {
+            if (i + 1 >= argc || !parse_ce(argv[i + 1], &ex->ce)) {
+                std::cerr << "Error: --csmc-is-ce requires ROUNDS,RUNS,ADAM_STEPS,LR" << std::endl;
+                return false;
+            }
+            ++i;
+        } else if (arg == "--csmc-formula" || arg == "--csmc-json" || arg == "--csmc-runs-csv") {
             if (i + 1 >= argc) {
                 std::cerr << "Error: " << arg << " requires a value" << std::endl;
                 return false;
@@ -118,6 +150,34 @@ int main(int argc, char *argv[]) {
     Extras ex;
     if (!handle_args(argc, argv, &filename, &seed, &st, &ex)) return 0;
     int rc;
+    if (ex.is) {
+        csmc_query q{};
+        int sims = st.simulations;
+        if (!ex.formula.empty()) {
+            char buf[512];
+            uint64_t n = 0;
+            rc = csmc_query_parse(filename.c_str(), ex.formula.c_str(), &q, buf, sizeof buf, &n);
+            if (rc != CSMC_OK) {
+                std::cerr << "Error: " << csmc_last_error() << std::endl;
+                return 0;
+            }
+            if (n > static_cast<uint64_t>(INT32_MAX)) {
+                std::cerr << "Error: the formula's run count " << n << " exceeds " << INT32_MAX << std::endl;
+                return 0;
+            }
+            if (n) sims = static_cast<int>(n);
+        } else {
+            q.kind = st.var_id == -1 ? CSMC_QUERY_LOCATION : CSMC_QUERY_VARIABLE;
+            q.var_id = st.var_id;
+            q.is_max = st.is_max ? 1 : 0;
+            q.is_estimate = st.is_estimate ? 1 : 0;
+            q.threshold = st.threshold;
+            q.horizon = st.time_bound;
+        }
+        rc = csmc_smc_is(filename.c_str(), seed, sims, &q, &ex.ce, ex.json.empty() ? nullptr : ex.json.c_str());
+        if (rc != CSMC_OK) std::cerr << "Error: " << csmc_last_error() << std::endl;
+        return 1;
+    }
     if (ex.formula.empty() && ex.json.empty() && ex.runs_csv.empty()) {
         rc = csmc_smc(filename.c_str(), seed, st.simulations, st.time_bound, st.threshold, st.var_id,
                       st.is_max ? 1 : 0, st.is_estimate ? 1 : 0, st.loc_query.c_str());

@@ -684,6 +684,20 @@ class Packer {
             h.n_rate_prog = static_cast<uint32_t>(rate_prog.size());
             h.n_inv_lit = static_cast<uint32_t>(inv_lit.size());
             if (h.n_rate_prog <= CSMC_MAX_RATE_PROGS) h.flags |= CSMC_NET_RATE_TABLE;
+            // whether some rate program reads a clock (then its value changes
+            // with every race step, not only with transitions)
+            bool reads_clock = false;
+            auto is_clock = [&](uint32_t v) { return v < nv && m_.var_kind_clock[v]; };
+            for (uint32_t hdl : rate_prog) {
+                const uint32_t tag = CSMC_H_TAG(hdl), pl = CSMC_H_PAYLOAD(hdl);
+                if (tag == CSMC_H_VAR) {
+                    reads_clock |= is_clock(pl);
+                } else if (tag == CSMC_H_PN || tag == CSMC_H_TREE) {
+                    for (size_t ip = pl + 1; ip < code_.size() && CSMC_INS_OP(code_[ip]) != CSMC_OP_END; ++ip)
+                        if (CSMC_INS_OP(code_[ip]) == CSMC_OP_PUSH_V) reads_clock |= is_clock(CSMC_INS_A(code_[ip]));
+                }
+            }
+            if (!reads_clock) h.flags |= CSMC_NET_RATE_NO_CLOCK;
         }
         std::vector<uint64_t> loc_desc;
         for (size_t i = 0; i < locs_.size(); ++i) {
@@ -725,7 +739,10 @@ class Packer {
                 }
                 d |= static_cast<uint64_t>(c << 8) << 32;
             }
-            if (ok && !cls.empty()) h.flags |= CSMC_NET_RACE_CLASSES;
+            if (ok && !cls.empty()) {
+                h.flags |= CSMC_NET_RACE_CLASSES;
+                h.n_classes = static_cast<uint32_t>(cls.size());
+            }
         }
         h.magic = CSMC_NET_MAGIC;
         h.version = CSMC_NET_VERSION;

@@ -85,12 +85,15 @@ typedef struct {
     uint32_t recv_chan_hi;   /* channels 32..63; bit 31 also stands for every channel >= 63 */
     uint32_t off_clock;      /* uint16 id per clock variable (n_clocks entries) */
     uint32_t off_loc_desc;   /* uint64 delay descriptor per location (CSMC_DESC_*) */
-    uint32_t reserved[2];
+    uint32_t n_classes;      /* race classes in use (with CSMC_NET_RACE_CLASSES; 0: not recorded) */
+    uint32_t reserved;
 } csmc_net_header; /* 160 bytes */
 
 /* Header flags. */
 #define CSMC_NET_RATE_TABLE 1u  /* rates resolved through loc_rate (see below) */
 #define CSMC_NET_RACE_CLASSES 2u /* delay descriptors carry race classes (see below) */
+#define CSMC_NET_RATE_NO_CLOCK 4u /* no rate program reads a clock: the rate table
+                                     changes only when a transition writes a variable */
 
 /* Rate slot of a location (loc_rate[]): bit 15 set -> index into the
  * per-step table of evaluated rate programs (rate_prog[]); clear -> index

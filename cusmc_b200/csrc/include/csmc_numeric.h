@@ -180,15 +180,11 @@ struct u32x4 {
     uint32_t x, y, z, w;
 };
 
+// 32 x 32 -> 64-bit product split into halves (one wide multiply).
 CSMC_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
-#ifdef __CUDA_ARCH__
-    lo = a * b;
-    hi = __umulhi(a, b);
-#else
     const uint64_t p = static_cast<uint64_t>(a) * static_cast<uint64_t>(b);
     lo = static_cast<uint32_t>(p);
     hi = static_cast<uint32_t>(p >> 32);
-#endif
 }
 
 CSMC_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
@@ -218,6 +214,74 @@ CSMC_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
 CSMC_HD u32x4 delay_block(uint64_t seed, uint64_t run, uint32_t step, uint32_t comp_group) {
     u32x4 c{step, comp_group, static_cast<uint32_t>(run), static_cast<uint32_t>(run >> 32)};
     return philox4x32_10(c, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+}
+
+// The delay blocks of one race step share every counter word but the
+// component group q: counter (step, q, run low, run high), key = seed.  The
+// parts of rounds 1-3 that depend only on the shared words are computed once
+// per step (philox_step); philox_block(q) finishes the block.  The integer
+// operations are those of philox4x32_10 regrouped, so the bits are equal.
+// Round keys: k0 + r * 0x9E3779B9, k1 + r * 0xBB67AE85 for rounds r = 0..9.
+struct PhiloxKeys {
+    uint32_t k0[10], k1[10];
+};
+
+CSMC_HD PhiloxKeys philox_keys(uint64_t seed) {
+    PhiloxKeys K;
+    uint32_t a = static_cast<uint32_t>(seed), b = static_cast<uint32_t>(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        K.k0[r] = a;
+        K.k1[r] = b;
+        a += 0x9E3779B9u;
+        b += 0xBB67AE85u;
+    }
+    return K;
+}
+
+struct PhiloxStep {
+    uint32_t a1;  // round 1: x = a1 ^ q
+    uint32_t c2;  // round 2: z = hi(M0 * x1) ^ c2
+    uint32_t d3;  // round 3: x = hi(M1 * z2) ^ d3
+    uint32_t b3;  // round 3: z = b3 ^ lo(M0 * x1)
+    uint32_t w3;  // round 3: w
+};
+
+CSMC_HD PhiloxStep philox_step(const PhiloxKeys &K, uint32_t step, uint64_t run) {
+    uint32_t h0, l0, h1, l1;
+    mulhilo32(0xD2511F53u, step, h0, l0);
+    mulhilo32(0xCD9E8D57u, static_cast<uint32_t>(run), h1, l1);
+    // after round 1: x1 = h1 ^ q ^ k0[0], y1 = l1, z1 = h0 ^ run_hi ^ k1[0], w1 = l0
+    const uint32_t y1 = l1, z1 = h0 ^ static_cast<uint32_t>(run >> 32) ^ K.k1[0], w1 = l0;
+    PhiloxStep s;
+    s.a1 = h1 ^ K.k0[0];
+    // round 2: the z1 product is shared; x2 and y2 are shared
+    uint32_t g1, g0;
+    mulhilo32(0xCD9E8D57u, z1, g1, g0);
+    const uint32_t x2 = g1 ^ y1 ^ K.k0[1], y2 = g0;
+    s.c2 = w1 ^ K.k1[1];
+    // round 3: the x2 product is shared
+    uint32_t p1, p0;
+    mulhilo32(0xD2511F53u, x2, p1, p0);
+    s.d3 = y2 ^ K.k0[2];
+    s.b3 = p1 ^ K.k1[2];
+    s.w3 = p0;
+    return s;
+}
+
+CSMC_HD u32x4 philox_block(const PhiloxKeys &K, const PhiloxStep &s, uint32_t q) {
+    uint32_t h0, l0, h1, l1;
+    mulhilo32(0xD2511F53u, s.a1 ^ q, h0, l0);         // round 2, the x1 product
+    const uint32_t z2 = h0 ^ s.c2, w2 = l0;
+    mulhilo32(0xCD9E8D57u, z2, h1, l1);               // round 3, the z2 product
+    u32x4 c{h1 ^ s.d3, l1, s.b3 ^ w2, s.w3};
+#pragma unroll
+    for (int r = 3; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+        c = u32x4{hi1 ^ c.y ^ K.k0[r], lo1, hi0 ^ c.w ^ K.k1[r], lo0};
+    }
+    return c;
 }
 
 CSMC_HD uint32_t word_of(const u32x4 &b, uint32_t i) {

@@ -34,13 +34,17 @@ struct NetLayout {
     uint32_t off_comp, off_loc, off_edge, off_guard, off_update, off_var, off_const, off_code;
     uint32_t off_loc_rate, off_inv_lit, off_rate_prog, off_clock, off_loc_desc;
     uint32_t n_comps, n_vars, n_rate_prog, flags, n_clocks, recv_lo, recv_hi;
+    uint32_t n_classes;  // race classes in use (CSMC_RACE_CLASSES when the blob does not record it)
+    uint32_t pad;
 };
 
 inline NetLayout layout_of(const csmc_net_header &h) {
+    const uint32_t ncls = (h.n_classes && h.n_classes <= CSMC_RACE_CLASSES) ? h.n_classes : CSMC_RACE_CLASSES;
     return NetLayout{h.off_comp,     h.off_loc,     h.off_edge,      h.off_guard,    h.off_update,
                      h.off_var,      h.off_const,   h.off_code,      h.off_loc_rate, h.off_inv_lit,
                      h.off_rate_prog, h.off_clock,  h.off_loc_desc,  h.n_comps,      h.n_vars,
-                     h.n_rate_prog,  h.flags,       h.n_clocks,      h.recv_chan_lo, h.recv_chan_hi};
+                     h.n_rate_prog,  h.flags,       h.n_clocks,      h.recv_chan_lo, h.recv_chan_hi,
+                     ncls,           0u};
 }
 
 struct SimParams {
@@ -67,6 +71,8 @@ struct SimParams {
     unsigned long long *scratch;  // [0] work counter [1] hits [2] steps [3] capped [4] errors
     uint8_t *state_global;        // thread-per-run kernel: per-CTA state slabs in global memory
                                   // (null: state in shared memory after the network)
+    PhiloxKeys keys;              // round keys of the seed (philox_keys(seed)): read from the
+                                  // parameter bank by the class-coded kernel
 };
 
 #define CSMC_SCRATCH_WORDS 8
@@ -85,6 +91,20 @@ int serial_launch(bool verify, bool slots, bool loc8, bool gstate, bool classes,
                   int block, size_t smem, void *stream);
 int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, bool classes, int block, size_t smem,
                            int *ctas);
+
+// Class-coded thread-per-run kernel (sim_coded.cuh): networks with race
+// classes, at most 256 components and at most 32 locations per automaton,
+// run state in shared memory.
+int coded_launch(bool verify, bool slots, const SimParams &p, int grid, int block, size_t smem, void *stream);
+int coded_max_active_ctas(bool verify, bool slots, int block, size_t smem, int *ctas);
+// Bytes of a T-thread state slab of the class-coded kernel (carve_coded_view).
+inline size_t coded_slab_bytes(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots, uint32_t T) {
+    size_t b = (4u * (2u * n_vars + n_rate_prog) * static_cast<size_t>(T) + 7u) & ~static_cast<size_t>(7);
+    b += 8u * 4u * CSMC_RACE_CLASSES * static_cast<size_t>(T);     // class keys: (largest, second) per chain
+    b += 4u * ((n_comps + 3u) / 4u) * static_cast<size_t>(T);        // location words
+    if (slots) b += 4u * n_comps * static_cast<size_t>(T);          // enabled-edge slot masks
+    return (b + 15u) & ~static_cast<size_t>(15);
+}
 
 // ---- Multi-network batch kernel (sim_batch.cuh) ---------------------------
 // One persistent launch simulates the runs of many (network, query) jobs.
@@ -112,7 +132,6 @@ struct BatchJob {
     uint64_t *digests;             // verification outputs (may be null)
     uint32_t *final_state;
     unsigned long long *counters;  // [0] hits [1] steps [2] capped
-    uint64_t pad;
 };
 static_assert(sizeof(BatchJob) % 16 == 0, "BatchJob is copied in 16-byte words");
 

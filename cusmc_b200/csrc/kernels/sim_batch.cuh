@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(
                 local = r - J.run_begin;
                 run = J.first_run + local;
                 const Net n = net_view(J.blob, J.net);
-                run_init<true, false>(n, J.net.n_comps, J.net.n_vars, rv, sc, J.var_id);
+                run_init<true>(n, J.net.n_comps, J.net.n_vars, rv, sc, J.var_id);
                 time = 0.0f;
                 step = 0;
             }
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(
             if (J.steps) J.steps[local] = step;
             if (VERIFY) {
                 if (J.digests) J.digests[local] = sc.digest;
-                if (J.final_state) run_final_state<false>(n, C, V, rv, J.final_state + local * (C + V));
+                if (J.final_state) run_final_state(n, C, V, rv, J.final_state + local * (C + V));
             }
             acc_hits += e.flag;
             acc_steps += step;

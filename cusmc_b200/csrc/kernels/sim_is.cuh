@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
 
             // pending broadcast receivers (serial, lane 0), then the rate table
             int moved = 0;
-            if (lane == 0) moved = run_receivers<false, SLOTS, LOC8>(n, C, V, rv, sc, p.seed, p.var_id, run, step);
+            if (lane == 0) moved = run_receivers<false, SLOTS>(n, C, V, rv, sc, p.seed, p.var_id, run, step);
             __syncwarp();
             stale = stale || __shfl_sync(kFullWarp, moved, 0) != 0;
             if (rate_table && stale) {
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
             if (lane == 0) {
                 uint32_t s0 = step;
                 float t0 = time;
-                took = run_commit<false, SLOTS, LOC8>(n, p.net.n_clocks, rv, sc, p.seed, p.var_id, run, s0, t0, win,
+                took = run_commit<false, SLOTS>(n, p.net.n_clocks, rv, sc, p.seed, p.var_id, run, s0, t0, win,
                                                       dmin);
             }
             __syncwarp();

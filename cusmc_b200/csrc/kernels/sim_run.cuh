@@ -80,8 +80,8 @@ static __device__ __forceinline__ RunView<LOC8> carve_run_view(uint8_t *st, uint
 
 // Run initialisation (simulation.cu:766-831): initial locations, slot
 // masks, initial variable values, query extremes.
-template <bool SLOTS, bool LOC8>
-static __device__ __forceinline__ void run_init(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+template <bool SLOTS, class RV>
+static __device__ __forceinline__ void run_init(const Net &n, uint32_t C, uint32_t V, const RV &rv,
                                                 RunScalars &sc, int var_id) {
     for (uint32_t c = 0; c < C; ++c) {
         rv.set_local(n, c, n.comp[c].init_local);
@@ -116,8 +116,8 @@ static __device__ __forceinline__ RunEnd run_end(const RunScalars &sc, float tim
 }
 
 // Final state for verification: local locations, then variable bits.
-template <bool LOC8>
-static __device__ __forceinline__ void run_final_state(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+template <class RV>
+static __device__ __forceinline__ void run_final_state(const Net &n, uint32_t C, uint32_t V, const RV &rv,
                                                        uint32_t *w) {
     for (uint32_t c = 0; c < C; ++c) w[c] = rv.loc(n, c) - n.comp[c].loc_begin;
     for (uint32_t v = 0; v < V; ++v) w[C + v] = f_bits(rv.vars[v]);
@@ -127,8 +127,8 @@ static __device__ __forceinline__ void run_final_state(const Net &n, uint32_t C,
 // simulation.cu:357-407): enabled sets from the state the sender left (the
 // snapshot), then transitions in component order on the live state.
 // Returns true when a receiver took an edge.
-template <bool VERIFY, bool SLOTS, bool LOC8>
-static __device__ __forceinline__ bool run_receivers(const Net &n, uint32_t C, uint32_t V, const RunView<LOC8> &rv,
+template <bool VERIFY, bool SLOTS, class RV>
+static __device__ __forceinline__ bool run_receivers(const Net &n, uint32_t C, uint32_t V, const RV &rv,
                                                      RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
                                                      uint32_t step) {
     if (sc.chan <= 0) return false;
@@ -163,8 +163,8 @@ static __device__ __forceinline__ bool run_receivers(const Net &n, uint32_t C, u
 // The race's outcome applied (simulation.cu:632-667, 876-882): clocks
 // advance by dmin, the winner takes an enabled edge, time advances.
 // Returns true when the winner took an edge.
-template <bool VERIFY, bool SLOTS, bool LOC8>
-static __device__ __forceinline__ bool run_commit(const Net &n, uint32_t n_clocks, const RunView<LOC8> &rv,
+template <bool VERIFY, bool SLOTS, class RV>
+static __device__ __forceinline__ bool run_commit(const Net &n, uint32_t n_clocks, const RV &rv,
                                                   RunScalars &sc, uint64_t seed, int var_id, uint64_t run,
                                                   uint32_t &step, float &time, uint32_t win, float dmin) {
     const uint32_t T = rv.T;
@@ -203,8 +203,8 @@ static __device__ __forceinline__ bool run_commit(const Net &n, uint32_t n_clock
 
 // The race over every component (simulation.cu:409-628): per-component
 // delays, minimum of (delay key, bit-reversed index).
-template <bool LOC8>
-static __device__ __forceinline__ void race_exact(const Net &n, uint32_t C, uint32_t bits, const RunView<LOC8> &rv,
+template <class RV>
+static __device__ __forceinline__ void race_exact(const Net &n, uint32_t C, uint32_t bits, const RV &rv,
                                                   uint64_t seed, uint64_t run, uint32_t step, unsigned long long &best,
                                                   float &bestd) {
     best = ~0ull;
@@ -248,8 +248,8 @@ static __device__ __forceinline__ void race_exact(const Net &n, uint32_t C, uint
 // when that cannot be ruled out from the two largest keys (or when a class's
 // 1/rate is not finite and positive and the class could take part in the
 // minimum) the function returns false and the caller runs race_exact.
-template <bool LOC8>
-static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, uint32_t bits, const RunView<LOC8> &rv,
+template <class RV>
+static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, uint32_t bits, const RV &rv,
                                                     uint64_t seed, uint64_t run, uint32_t step,
                                                     unsigned long long &best, float &bestd) {
     const uint32_t T = rv.T;
@@ -335,13 +335,13 @@ static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, ui
 // One step of a run: pending broadcast receivers, the per-step rate table,
 // the race, the clock advance and the winner's transition, the time update.
 // CLASSES: the network's descriptors carry race classes (C <= 256).
-template <bool VERIFY, bool SLOTS, bool LOC8, bool CLASSES = false>
+template <bool VERIFY, bool SLOTS, bool CLASSES, class RV>
 static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32_t V, uint32_t P, uint32_t n_clocks,
-                                                bool rate_table, const RunView<LOC8> &rv, RunScalars &sc,
+                                                bool rate_table, const RV &rv, RunScalars &sc,
                                                 uint64_t seed, int var_id, uint64_t run, uint32_t &step,
                                                 float &time) {
     const uint32_t bits = ceil_log2(C);
-    run_receivers<VERIFY, SLOTS, LOC8>(n, C, V, rv, sc, seed, var_id, run, step);
+    run_receivers<VERIFY, SLOTS>(n, C, V, rv, sc, seed, var_id, run, step);
 
     // ---- distinct rate programs, once per step
     if (rate_table)
@@ -351,13 +351,13 @@ static __device__ __forceinline__ void run_step(const Net &n, uint32_t C, uint32
     unsigned long long best;
     float bestd;
     if (CLASSES) {
-        if (!race_classes<LOC8>(n, C, bits, rv, seed, run, step, best, bestd))
-            race_exact<LOC8>(n, C, bits, rv, seed, run, step, best, bestd);
+        if (!race_classes(n, C, bits, rv, seed, run, step, best, bestd))
+            race_exact(n, C, bits, rv, seed, run, step, best, bestd);
     } else {
-        race_exact<LOC8>(n, C, bits, rv, seed, run, step, best, bestd);
+        race_exact(n, C, bits, rv, seed, run, step, best, bestd);
     }
     const uint32_t win = bitrev_bits(static_cast<uint32_t>(best & 0xffffffffull), bits);
-    run_commit<VERIFY, SLOTS, LOC8>(n, n_clocks, rv, sc, seed, var_id, run, step, time, win, bestd);
+    run_commit<VERIFY, SLOTS>(n, n_clocks, rv, sc, seed, var_id, run, step, time, win, bestd);
 }
 
 }  // namespace detail

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
                 if (ridx >= p.n_runs) break;
                 have = true;
                 run = p.first_run + ridx;
-                run_init<SLOTS, LOC8>(n, C, V, rv, sc, p.var_id);
+                run_init<SLOTS>(n, C, V, rv, sc, p.var_id);
                 time = 0.0f;
                 step = 0;
             }
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             if (p.steps) p.steps[ridx] = step;
             if (VERIFY) {
                 if (p.digests) p.digests[ridx] = sc.digest;
-                if (p.final_state) run_final_state<LOC8>(n, C, V, rv, p.final_state + ridx * (C + V));
+                if (p.final_state) run_final_state(n, C, V, rv, p.final_state + ridx * (C + V));
             }
             acc_hits += e.flag;
             acc_steps += step;
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(128, CSMC_SERIAL_MIN_CTAS_PER_SM) serial_kerne
             continue;
         }
 
-        run_step<VERIFY, SLOTS, LOC8, CLASSES>(n, C, V, P, p.net.n_clocks, rate_table, rv, sc, p.seed, p.var_id, run,
+        run_step<VERIFY, SLOTS, CLASSES>(n, C, V, P, p.net.n_clocks, rate_table, rv, sc, p.seed, p.var_id, run,
                                                step, time);
     }
     // lanes leave the loop at different times; aggregate per lane

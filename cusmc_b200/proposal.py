@@ -202,31 +202,53 @@ class Elite:
 def select_elite(values: np.ndarray, logw: np.ndarray, steps: np.ndarray, threshold: float, is_max: bool = True,
                  rho: float = 0.1, max_rows: int = 40_000_000) -> Elite:
     """Multi-level CE selection for the goal value > threshold (max query) or
-    value < threshold (min query): the level is the (1 - rho)-quantile of the
-    runs' scores (the value, negated for a min query), capped at the goal;
-    the elite are the runs at or beyond the level (strictly beyond the goal
-    once the level reaches it), weighted by their likelihood ratios.  Runs
-    are kept heaviest first while their rows (4 per step) fit in max_rows,
-    and at least one run is kept."""
-    score = np.asarray(values, np.float64) if is_max else -np.asarray(values, np.float64)
-    goal = threshold if is_max else -threshold
-    n = len(score)
-    level = min(goal + 1e-9, float(np.quantile(score, 1.0 - rho)))
-    elite = np.nonzero(score >= level)[0] if level <= goal else np.nonzero(score > goal)[0]
-    if len(elite) == 0:
-        elite = np.argsort(score)[-max(1, int(rho * n)):]
-    lw = np.asarray(logw, np.float64)[elite]
-    w = np.exp(lw - lw.max())
-    w = w / w.sum()
-    st = np.asarray(steps).astype(np.int64)
-    order = np.argsort(-w)
-    keep = order[np.cumsum(4 * st[elite][order]) <= max_rows]
-    if len(keep) == 0:
-        keep = order[:1]
-    elite, w = elite[keep], w[keep]
-    w = (w / w.sum()).astype(np.float32)
-    offs = np.concatenate([[0], np.cumsum(4 * st[elite])[:-1]]).astype(np.uint64)
-    return Elite(level if is_max else -level, elite, w, offs, int((4 * st[elite]).sum()), level > goal)
+    value < threshold (min query), by the library's host routine
+    csmc_ce_select (the C++ training loop uses the same one): the level is
+    the (1 - rho)-quantile of the runs' scores (the value, negated for a min
+    query; linear interpolation between order statistics), capped at the
+    goal; the elite are the runs at or beyond the level (strictly beyond the
+    goal once the level reaches it), weighted by their likelihood ratios.
+    Runs are kept heaviest first while their rows (4 per step) fit in
+    max_rows, and at least one run is kept."""
+    values = np.ascontiguousarray(values, np.float64)
+    logw = np.ascontiguousarray(logw, np.float64)
+    steps = np.ascontiguousarray(steps, np.uint32)
+    n = len(values)
+    elite = np.zeros(n, np.uint64)
+    weights = np.zeros(n, np.float32)
+    offs = np.zeros(n, np.uint64)
+    ne, nr, lev, at = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double(), ctypes.c_int32()
+    check(lib().csmc_ce_select(values.ctypes.data, logw.ctypes.data, steps.ctypes.data, n, float(threshold),
+                               1 if is_max else 0, float(rho), int(max_rows), elite.ctypes.data, weights.ctypes.data,
+                               offs.ctypes.data, ctypes.byref(ne), ctypes.byref(nr), ctypes.byref(lev),
+                               ctypes.byref(at)))
+    k = ne.value
+    return Elite(lev.value, elite[:k].astype(np.int64), weights[:k].copy(), offs[:k].copy(), int(nr.value),
+                 bool(at.value))
+
+
+def init_c(seed: int = 0) -> "Proposal":
+    """The library's initial proposal (csmc_mlp_init; what the CLI trains from)."""
+    v = np.zeros(GRAD_FLOATS, np.float32)
+    check(lib().csmc_mlp_init(seed & (2**64 - 1), v.ctypes.data))
+    return Proposal.from_vector(v)
+
+
+def train_c(net, query: Query, seed: int = 1, init: "Proposal | None" = None, rounds: int = 10,
+            runs_per_round: int = 100_000, rho: float = 0.1, adam_steps: int = 30, lr: float = 3e-3,
+            max_rows: int = 40_000_000, settle: int = 0):
+    """CE training through the C ABI (csmc_is_train): the same method as
+    train(), run by the library.  Returns (Proposal, list of round dicts)."""
+    from ._native import CeConfig, CeRound
+    x0 = (init or Proposal.init(0)).vector()
+    cfg = CeConfig(rounds=rounds, adam_steps=adam_steps, runs_per_round=runs_per_round, max_rows=max_rows, rho=rho,
+                   lr=lr, settle=settle)
+    out = np.zeros(GRAD_FLOATS, np.float32)
+    log = (CeRound * rounds)()
+    done = ctypes.c_int32()
+    check(lib().csmc_is_train(net._h, ctypes.byref(query), seed & (2**64 - 1), ctypes.byref(cfg), x0.ctypes.data,
+                              out.ctypes.data, None, log, rounds, ctypes.byref(done)))
+    return Proposal.from_vector(out), [log[i].as_dict() for i in range(done.value)]
 
 
 def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: int = 100_000, rho: float = 0.1,

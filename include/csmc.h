@@ -73,7 +73,8 @@ typedef struct {
     int32_t comps_per_lane; /* components per lane */
     int32_t runs_per_cta;   /* runs in flight per CTA */
     int32_t family;         /* 0 lane-group kernel, 1 thread-per-run kernel, 2 thread-per-run with
-                               the network in global memory (batch kernel, one job) */
+                               the network in global memory (batch kernel, one job), 3 importance
+                               sampling (one warp per run), 4 class-coded thread-per-run kernel */
 } csmc_result;
 
 /* Thread-local message of the last failure on this thread. */
@@ -169,8 +170,11 @@ int csmc_plan(const csmc_net *net, int32_t *lanes_per_run, int32_t *comps_per_la
  * family 0 = lane groups of lanes_per_run lanes (power of two <= 32) with
  * comps_per_lane components each; family 2 = one thread per run with the
  * network and run state in global memory (networks larger than shared
- * memory); family 1 = one thread per run (lanes and
- * comps_per_lane are ignored).  threads_per_cta: CTA size. */
+ * memory); family 1 = one thread per run; family 4 = one thread per run with
+ * class-coded locations (networks with race classes, at most 256 components
+ * and 32 locations per automaton; the default for them).  For families 1, 2
+ * and 4 lanes and comps_per_lane are ignored.  threads_per_cta: CTA size.
+ * Every family gives the same per-run results. */
 int csmc_set_plan(csmc_net *net, int32_t family, int32_t lanes_per_run, int32_t comps_per_lane,
                   int32_t threads_per_cta);
 
@@ -290,6 +294,84 @@ int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, floa
 int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
                   void *stream);
 
+/* ---- Cross-entropy training of the proposal ---------------------------
+ * No counterpart in the reference.  The reference's entry point for a run
+ * of the statistical model checker is smc() (smc.cuh:14, smc.cu:283-491);
+ * these entry points sit beside it for the learned importance-sampling
+ * method, so C/C++ hosts and the CLI (--csmc-is) can train without Python.
+ *
+ * Parameters cross the ABI as the FP32 master vector of CSMC_MLP_GRAD_FLOATS
+ * floats: w1[64][16], b1[64], w2[64][64], b2[64], w3[64], b3. */
+typedef struct {
+    int32_t rounds;          /* maximum CE rounds (>= 1) */
+    int32_t adam_steps;      /* Adam steps per round (>= 1), on the round's rows */
+    uint64_t runs_per_round; /* runs simulated under the proposal per round */
+    uint64_t max_rows;       /* cap on a round's training rows (4 per step of an elite run) */
+    double rho;              /* elite fraction, in (0, 1) */
+    double lr;               /* Adam step size (beta1 0.9, beta2 0.999, eps 1e-8) */
+    int32_t settle;          /* stop after this many consecutive rounds whose level was the goal (0: never) */
+    int32_t pad;
+} csmc_ce_config;
+
+typedef struct {
+    int32_t round;           /* 0-based */
+    int32_t elite;           /* elite runs replayed */
+    uint64_t rows;           /* training rows */
+    double level;            /* the round's level (the goal once at_goal) */
+    double j_start, j_end;   /* CE objective before the first and after the last Adam step */
+    double estimate;         /* the round's importance-sampling estimate */
+    uint64_t hits, capped;   /* runs at the goal; runs stopped by max_steps */
+    double mean_steps;       /* race steps per run */
+    double kernel_ms;        /* simulation kernel time of the round's runs */
+    double run_s, trace_s, adam_s; /* host seconds: runs + selection, replay, Adam steps */
+    int32_t at_goal;         /* 1 when the level was the goal */
+    int32_t pad;
+} csmc_ce_round;
+
+/* Multi-level CE selection of one round (host only).  score = value (max
+ * query) or -value (min query); goal = threshold (or -threshold).  The level
+ * is min(goal + 1e-9, q), q the (1 - rho)-quantile of the scores with linear
+ * interpolation between order statistics (sorted[lo] + (sorted[lo+1] -
+ * sorted[lo]) * (h - lo), h = (n - 1)(1 - rho)).  Elite: runs with score >=
+ * level, or score > goal once the level is the goal; if none, the
+ * max(1, floor(rho n)) highest-scoring runs.  Weights exp(logw - max logw),
+ * normalised; runs are kept heaviest first while their rows (4 per step)
+ * total at most max_rows (at least one run), and the kept weights are
+ * normalised again.  Outputs (capacity n each): elite run indices,
+ * weights (float), row_offset (exclusive prefix sums of 4 * steps, in the
+ * kept order); *n_elite, *n_rows, *level (in value units) and *at_goal. */
+int csmc_ce_select(const double *values, const double *logw, const uint32_t *steps, uint64_t n, double threshold,
+                   int32_t is_max, double rho, uint64_t max_rows, uint64_t *elite, float *weights,
+                   uint64_t *row_offset, uint64_t *n_elite, uint64_t *n_rows, double *level, int32_t *at_goal);
+
+/* FP32 master vector -> the CSMC_MLP_PARAM_BYTES parameter block (BF16
+ * weight matrices, round to nearest even). */
+int csmc_mlp_pack(const float *master, void *params);
+
+/* Initial master vector: w1 ~ N(0, 2/10) on the 10 used inputs, w2 ~
+ * N(0, 2/64) (Box-Muller over Philox4x32-10 draws keyed by seed), biases and
+ * the output layer 0, so theta = 0 (the proposal starts as the nominal model). */
+int csmc_mlp_init(uint64_t seed, float *master);
+
+/* CE training on the GPU: per round, runs_per_round runs under the current
+ * proposal (runs (k + 1) * 10^7 .. of the stream for round k), the elite
+ * selection above, their replay into rows and adam_steps Adam ascents of
+ * J = sum (b theta - a e^theta) with the tensor-core gradient.  init and
+ * trained are master vectors; params_out (may be NULL) receives the packed
+ * trained parameters; log (may be NULL, log_cap entries) one entry per
+ * round; *rounds_done the rounds run.  Needs a variable query. */
+int csmc_is_train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_config *cfg, const float *init,
+                  float *trained, void *params_out, csmc_ce_round *log, int32_t log_cap, int32_t *rounds_done);
+
+/* smc() (smc.cuh:14, smc.cu:283-491) with the learned importance-sampling
+ * estimate of a variable probability query (IS_ESTIMATE = 0): the settings
+ * report, CE training from csmc_mlp_init(seed) with cfg, then sims weighted
+ * runs; prints "Result:" with the estimate, its 95% confidence interval and
+ * the timing lines, and writes json_path (may be NULL) with the same.  This
+ * is the CLI's --csmc-is. */
+int csmc_smc_is(const char *model_path, int seed, int sims, const csmc_query *q, const csmc_ce_config *cfg,
+                const char *json_path);
+
 /* ---- Numeric primitives ----------------------------------------------------
  * No counterpart in the reference, whose random stream is curand XORWOW
  * (simulation/simulation.cu:756-760) and whose logarithm is the hardware
@@ -307,7 +389,10 @@ int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *
  *   CSMC_NUM_POW_F64       a, b: f64[n] -> f64 a^b (the model language's '^')
  *   CSMC_NUM_EXP2_F32      a: f32[n] -> f32 2^a (proposal network)
  *   CSMC_NUM_GELU_F32      a: f32[n] -> f32 GELU (tanh form)
- *   CSMC_NUM_GELU_GRAD_F32 a: f32[n] -> f32 GELU' */
+ *   CSMC_NUM_GELU_GRAD_F32 a: f32[n] -> f32 GELU'
+ *   CSMC_NUM_PHILOX_STEP   as CSMC_NUM_PHILOX, through the per-step
+ *                          factorisation the simulation kernels use
+ *                          (counter = step, component group, run low, run high) */
 #define CSMC_NUM_PHILOX 0
 #define CSMC_NUM_EXP_DELAY 1
 #define CSMC_NUM_LOG2_F32 2
@@ -317,6 +402,7 @@ int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *
 #define CSMC_NUM_EXP2_F32 6
 #define CSMC_NUM_GELU_F32 7
 #define CSMC_NUM_GELU_GRAD_F32 8
+#define CSMC_NUM_PHILOX_STEP 9
 int csmc_numeric_eval(int32_t fn, const void *a, const void *b, uint64_t n, void *out, void *stream);
 
 /* Measures the shared-memory bandwidth of the current device (no

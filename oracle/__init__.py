@@ -140,7 +140,7 @@ def mlp_grad(params: bytes, rows: np.ndarray):
 # ---- numeric primitives -----------------------------------------------------
 
 _NUM_OUT = {0: np.uint32, 1: np.float32, 2: np.float32, 3: np.float64, 4: np.float64, 5: np.float64,
-            6: np.float32, 7: np.float32, 8: np.float32}
+            6: np.float32, 7: np.float32, 8: np.float32, 9: np.uint32}
 
 
 def numeric(fn: int, a, b=None) -> np.ndarray:
@@ -149,7 +149,7 @@ def numeric(fn: int, a, b=None) -> np.ndarray:
     a = np.ascontiguousarray(a)
     b = None if b is None else np.ascontiguousarray(b)
     n = a.shape[0]
-    out = np.zeros((n, 4) if fn == 0 else n, dtype=_NUM_OUT[fn])
+    out = np.zeros((n, 4) if fn in (0, 9) else n, dtype=_NUM_OUT[fn])
     rc = lib().oracle_numeric_eval(fn, a.ctypes.data, None if b is None else b.ctypes.data, n, out.ctypes.data)
     if rc != 0:
         raise RuntimeError("oracle: " + lib().oracle_last_error().decode())

@@ -472,6 +472,19 @@ int oracle_numeric_eval(int32_t fn, const void *a, const void *b, uint64_t n, vo
             o[3] = r.w;
             break;
         }
+        case CSMC_NUM_PHILOX_STEP: {
+            const uint32_t *c = static_cast<const uint32_t *>(a) + 4 * i;
+            const uint32_t *k = static_cast<const uint32_t *>(b) + 2 * i;
+            const csmc::PhiloxKeys K = csmc::philox_keys(static_cast<uint64_t>(k[0]) | (static_cast<uint64_t>(k[1]) << 32));
+            const csmc::PhiloxStep S = csmc::philox_step(K, c[0], static_cast<uint64_t>(c[2]) | (static_cast<uint64_t>(c[3]) << 32));
+            const csmc::u32x4 r = csmc::philox_block(K, S, c[1]);
+            uint32_t *o = static_cast<uint32_t *>(out) + 4 * i;
+            o[0] = r.x;
+            o[1] = r.y;
+            o[2] = r.z;
+            o[3] = r.w;
+            break;
+        }
         case CSMC_NUM_EXP_DELAY:
             static_cast<float *>(out)[i] =
                 csmc::exp_delay(static_cast<const uint32_t *>(a)[i], static_cast<const float *>(b)[i]);

@@ -69,3 +69,40 @@ def test_weights_stay_finite_for_tiny_likelihood_ratios():
     values, logw, steps = _round()
     e = select_elite(values, logw - 5000.0, steps, threshold=150.0)
     assert np.all(np.isfinite(e.weights)) and abs(float(e.weights.sum()) - 1.0) < 1e-5
+
+
+def test_library_init_and_pack():
+    """csmc_mlp_init starts at theta = 0 (zero output layer, zero biases);
+    csmc_mlp_pack packs a master vector as Proposal.pack does (host code of
+    the library, no GPU)."""
+    import ctypes
+    import math
+    from cusmc_b200 import _native
+    from cusmc_b200 import proposal as P
+    p = P.init_c(7)
+    assert not p.w3.any() and p.b3 == 0.0 and not p.b1.any() and not p.b2.any() and not p.w1[:, 10:].any()
+    assert 0.5 < float(np.std(p.w1[:, :10])) / math.sqrt(0.2) < 1.5
+    assert 0.8 < float(np.std(p.w2)) / math.sqrt(2.0 / 64) < 1.2
+    assert np.array_equal(P.init_c(7).vector(), p.vector()) and not np.array_equal(P.init_c(8).vector(), p.vector())
+    r = P.Proposal.init(3)
+    rng = np.random.default_rng(5)
+    r.w3 = rng.standard_normal(64).astype(np.float32)
+    r.b3 = 0.25
+    r.b1 = rng.standard_normal(64).astype(np.float32)
+    buf = ctypes.create_string_buffer(P.PARAM_BYTES)
+    x = r.vector()
+    _native.check(_native.lib().csmc_mlp_pack(x.ctypes.data, buf))
+    assert buf.raw == r.pack()
+
+
+def test_selection_fallback_and_min_query():
+    """No run reaches the level (all scores equal to the quantile is not
+    possible here): the highest-scoring runs are taken; a min query negates
+    the scores and reports the level in value units."""
+    values = np.array([5.0, 1.0, 3.0, 2.0, 4.0] * 40)
+    logw = np.zeros(values.size)
+    steps = np.full(values.size, 10, np.uint32)
+    e = select_elite(values, logw, steps, threshold=2.5, is_max=False, rho=0.1)
+    assert e.at_goal and np.all(values[e.runs] < 2.5)
+    assert e.level == pytest.approx(2.5 - 1e-9)
+    assert abs(float(e.weights.sum()) - 1.0) < 1e-6

@@ -1,0 +1,93 @@
+"""The drop-in CLI against the reference cuSMC binary, run on the same
+model file and query: the stdout report must be the same line for line
+(main.cu:39-110, smc.cu:317,358-372,402, simulation/statistics.cuh:126-169),
+except for the run-dependent numbers in the result and timing lines, and
+the ../results5.csv each program writes must have the same header row and
+row keys (simulation/write_csv.cu:15-98).  The two estimates must also agree
+within Chernoff-Hoeffding bounds.
+
+The reference binaries are built from the reference sources by
+oracle/ref/Makefile (oracle/_ref/cusmc_ref_v<N>, MAX_VARIABLES = N); the
+test is skipped where they were not built.
+"""
+import csv
+import math
+import os
+import re
+import subprocess
+
+import pytest
+
+from cusmc_b200 import netgen
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "cusmc_b200", "bin", "cusmc")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+# lines whose numbers depend on the runs or the clock; every other line must
+# be byte-identical
+VOLATILE = ("Result: ", "Number of hits: ", "The answer to ", "Time taken: ")
+NUMBER = re.compile(r"[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?")
+
+CASES = [
+    # name, workload, -q arguments (SIMS T THRESH VAR_ID IS_MAX IS_ESTIMATE LOC_QUERY)
+    ("epidemic_var", lambda: netgen.epidemic(n_agents=30), ["4096", "100", "14", "3", "1", "0", ""]),
+    ("mutex_loc", lambda: netgen.mutex(8), ["4096", "40", "0", "-1", "1", "0", "P0.cs"]),
+    ("random_estimate", lambda: netgen.random_network(2), ["4096", "100", "7", "0", "1", "1", ""]),
+]
+
+
+def _reference_binary(n_vars):
+    for v in (8, 16, 64, 512):
+        if v >= n_vars:
+            path = os.path.join(REF_DIR, f"cusmc_ref_v{v}")
+            return path if os.path.exists(path) else None
+    return None
+
+
+def _masked(line):
+    return NUMBER.sub("#", line) if line.startswith(VOLATILE) else line
+
+
+def _result_of(stdout):
+    m = re.search(r"^Result: (\S+)", stdout, re.M)
+    if m:
+        return float(m.group(1))
+    m = re.search(r"^The answer to .* is (\S+)$", stdout, re.M)
+    return float(m.group(1)) if m else None
+
+
+@pytest.mark.parametrize("name,make,qargs", CASES, ids=[c[0] for c in CASES])
+def test_cli_report_and_csv_match_the_reference_binary(tmp_path, name, make, qargs):
+    w = make()
+    ref = _reference_binary(w.n_vars)
+    if ref is None:
+        pytest.skip("reference binary not built (oracle/ref/Makefile needs the reference checkout)")
+    model = w.write(str(tmp_path / f"{name}.xml"))
+    outs = {}
+    for who, exe in (("ref", ref), ("ours", CLI)):
+        run = tmp_path / who / "run"
+        run.mkdir(parents=True)
+        p = subprocess.run([exe, "-m", model, "-s", "11", "-q", *qargs], cwd=run, capture_output=True, text=True,
+                           timeout=600)
+        rows = list(csv.reader(open(tmp_path / who / "results5.csv"), delimiter=";"))
+        outs[who] = (p, rows)
+    (pr, rows_r), (po, rows_o) = outs["ref"], outs["ours"]
+    assert po.returncode == pr.returncode == 1, (pr.stderr, po.stderr)
+    ref_lines = [_masked(x) for x in pr.stdout.splitlines()]
+    our_lines = [_masked(x) for x in po.stdout.splitlines()]
+    assert our_lines == ref_lines
+    assert rows_o[0] == rows_r[0]
+    assert [r[0] for r in rows_o] == [r[0] for r in rows_r]
+    assert [len(r) for r in rows_o] == [len(r) for r in rows_r]
+    # the estimates agree within the two Chernoff-Hoeffding bounds (delta 1e-3)
+    n = int(qargs[0])
+    eps = math.sqrt(math.log(2 / 1e-3) / (2 * n))
+    a, b = _result_of(pr.stdout), _result_of(po.stdout)
+    assert a is not None and b is not None
+    if qargs[5] == "1":  # estimate of the mean maximum: scale the bound by the value range
+        assert abs(a - b) <= 2 * eps * 16
+    else:
+        assert abs(a - b) <= 2 * eps

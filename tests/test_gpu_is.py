@@ -210,3 +210,27 @@ def test_ce_training_lowers_the_error_of_a_rare_event_estimate():
     # the untrained proposal is plain SMC; the trained one is much tighter at equal runs
     assert h_is < 0.5 * h_is0 if h_is0 > 0 else h_is < p_is
     assert abs(p_is - p_plain) < 1.5 * (h_is + h_plain), (p_is, h_is, p_plain, h_plain)
+
+
+def test_c_abi_training_equals_the_python_training():
+    """csmc_is_train (the CE loop in the library, for hosts without Python)
+    and proposal.train (the loop in Python: its own Adam in numpy, its own
+    BF16 packing) end with the same parameters bit for bit from the same
+    initial parameters, and log the same rounds.  Both use the library's
+    elite selection (csmc_ce_select) and the same kernels."""
+    w = netgen.epidemic()
+    net = api.Network(_blob(w))
+    try:
+        q = api.variable_query(w.var_id, 75, threshold=94, is_max=True)
+        cfg = dict(rounds=3, runs_per_round=3000, adam_steps=6, lr=3e-2, max_rows=300_000, settle=0)
+        prop_py, log_py = P.train(net, q, seed=4, init_seed=0, **cfg)
+        prop_c, log_c = P.train_c(net, q, seed=4, init=P.Proposal.init(0), **cfg)
+    finally:
+        net.close()
+    assert np.array_equal(prop_py.vector().view(np.uint32), prop_c.vector().view(np.uint32))
+    assert len(log_py.rounds) == len(log_c) == 3
+    for a, b in zip(log_py.rounds, log_c):
+        assert a["elite"] == b["elite"] and a["rows"] == b["rows"] and a["level"] == b["level"]
+        assert a["J_start"] == b["j_start"] and a["J_end"] == b["j_end"] and a["hits"] == b["hits"]
+    assert prop_c.pack() == P.Proposal.from_vector(prop_c.vector()).pack()
+
