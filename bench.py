@@ -152,12 +152,14 @@ def workload_blob(name):
     return w, path, blob, q
 
 
-def profile_traffic_per_run(name):
-    """DRAM bytes (read + write) per run of the simulation kernel, from the ncu
-    capture summarised in profiles/ (a smaller launch of the same kernel and
-    network, scaled by runs): the line `dram_bytes_per_run = X`."""
-    p = os.path.join(ROOT, "profiles", f"serial_kernel_{name}.md")
-    if not os.path.exists(p):
+def profile_traffic_per_run(name, family):
+    """DRAM bytes (read + write) per run of the simulation kernel the plan
+    uses, from the ncu capture summarised in profiles/ (a smaller launch of
+    the same kernel and network, scaled by runs): the line
+    `dram_bytes_per_run = X` of profiles/<kernel>_<workload>.md."""
+    kernel = {4: "coded_kernel", 1: "serial_kernel"}.get(family)
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{name}.md")
+    if kernel is None or not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
@@ -279,7 +281,7 @@ def run_ours(args):
     # 8-byte value per run written, the network read once
     alg_bytes = 9 * n + len(blob)
     achieved = alg_bytes / (launch_ms / 1000.0) / 1e9
-    traffic_per_run = profile_traffic_per_run(args.workload)
+    traffic_per_run = profile_traffic_per_run(args.workload, r.family)
     # the kernel is bound by instruction issue and shared-memory access, not
     # HBM: one component-step (one component's part in one race) touches
     # 32 B of run state and network records in shared memory
@@ -475,8 +477,13 @@ def run_batch(args):
     batch = api.Batch(jobs)
     t_tune = time.perf_counter()
     geometry = batch.autotune(probe_fraction=0.02)
+    tuned_min = batch.group_comps()[0]
+    thresholds = [int(x) for x in str(args.batch_group_comps).split(",")]
+    if thresholds[0] >= 0:
+        batch.set_group_comps(thresholds[0])
+    group = batch.group_comps()
     t_tune = time.perf_counter() - t_tune
-    progress(f"autotuned {geometry}")
+    progress(f"autotuned {geometry} (warp-per-run from {tuned_min} components), using {group}")
     for _ in range(args.warmup):
         r0 = batch.run(use_graph=True)
         progress(f"warm-up batch {r0[0].kernel_ms:.1f} ms")
@@ -487,6 +494,15 @@ def run_batch(args):
         res = batch.run(use_graph=True)
         batch_ms.append(res[0].kernel_ms)
     clocks = sampler.stop()
+    # other warp-per-run thresholds, one timed pass each (results must not change)
+    sweep = []
+    for m in thresholds[1:]:
+        batch.set_group_comps(m)
+        r1 = batch.run(use_graph=True)
+        same_m = all(a.hits == b.hits and a.steps == b.steps and a.sum == b.sum for a, b in zip(res, r1))
+        sweep.append({"min_comps": m, "warp_per_run_jobs": batch.group_comps()[1], "ms": r1[0].kernel_ms,
+                      "runs_per_s": total / (r1[0].kernel_ms / 1000.0), "results_identical": same_m})
+        progress(f"warp-per-run from {m} components: {r1[0].kernel_ms:.1f} ms")
     # the same jobs as sequential launches
     seq_ms = []
     seq_res = None
@@ -508,7 +524,10 @@ def run_batch(args):
             "data": "synthetic (64 seeded generated networks)",
             "config": {"workload": f"batch_64 (random networks, seeds 1000..1063; each run budget / {scale})",
                        "runs_per_step": total,
-                       "threads_per_cta": geometry[0], "ctas_per_sm": geometry[1], "graph": True},
+                       "threads_per_cta": geometry[0], "ctas_per_sm": geometry[1], "graph": True,
+                       "warp_per_run_min_comps": group[0], "warp_per_run_jobs": group[1],
+                       "autotuned_min_comps": tuned_min},
+            "group_sweep": sweep,
             "sequential": {"value": seq_value, "unit": "runs/s", "ms_per_step": sum(seq_ms) / len(seq_ms)},
             "speedup_vs_sequential": value / seq_value, "results_identical_to_sequential": same,
             "autotune_s": t_tune, "clocks": clocks, "gpu_launches": 2 * args.steps}
@@ -529,10 +548,20 @@ def run_rare_is(args):
     torch.cuda.set_device(local)
     w = netgen.epidemic()
     net = api.Network(_blob_of(w))
+    if args.is_tc:
+        P.set_inference(net, True)
+    if args.is_warp:
+        P.set_kernel(net, 3)
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
+    ce = dict(IS_CE)
+    for key, val in (("rounds", args.ce_rounds), ("runs_per_round", args.ce_runs), ("adam_steps", args.ce_steps)):
+        if val:
+            ce[key] = val
+    if args.ce_rounds:
+        ce["settle"] = 0  # exactly the requested number of rounds
     t0 = time.perf_counter()
-    prop, log = P.train(net, q, seed=1, **IS_CE)
+    prop, log = P.train(net, q, seed=1, **ce)
     train_s = time.perf_counter() - t0
     # importance sampling until the 95% CI half-width is 10% of the estimate
     chunk = IS_CHUNK
@@ -576,8 +605,10 @@ def run_rare_is(args):
             "value": train_s + is_s, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16 network / f32 accumulation / f64 log-weights", "data": "synthetic",
-            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1})", "ce": IS_CE,
-                       "sample_chunk": chunk, "inference": "cuda cores (oracle order)"},
+            "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1})", "ce": ce,
+                       "sample_chunk": chunk,
+                       "inference": "tensor cores (mma.sync bf16)" if args.is_tc else "cuda cores (oracle order)",
+                       "kernel": "one thread per run" if r.family == 5 else "one warp per run"},
             "is": {"estimate": p, "ci_half": half, "runs": n, "train_s": train_s, "sample_s": is_s},
             "plain": {"estimate": p_plain, "ci_half": half_plain, "runs": plain_n, "runs_per_s": plain_rate,
                       "runs_for_10pct": need_plain, "seconds_for_10pct": plain_to_10},
@@ -600,6 +631,10 @@ def run_is_kernel(args):
     torch.cuda.set_device(local)
     w = netgen.epidemic()
     net = api.Network(_blob_of(w))
+    if args.is_tc:
+        P.set_inference(net, True)
+    if args.is_warp:
+        P.set_kernel(net, 3)
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
     prop, log = P.train(net, q, seed=1, **IS_CE)
@@ -609,10 +644,12 @@ def run_is_kernel(args):
         P.is_run(net, q, params, 9, n, 5_000_000_000 + i * n)
     ms = []
     steps = 0
+    family = None
     for i in range(args.steps):
         r = P.is_run(net, q, params, 9, n, 6_000_000_000 + i * n)
         ms.append(r.kernel_ms)
         steps += r.steps
+        family = r.family
     net.close()
     t = sum(ms) / 1000.0
     line = {"metric": "runs/s of the importance-sampling kernel under a trained proposal", "value": n * args.steps / t,
@@ -620,6 +657,8 @@ def run_is_kernel(args):
             "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 network evaluation / f64 log-weights", "data": "synthetic",
             "config": {"workload": f"epidemic_100, Pr[<={T}](<> R>={thr + 1}), {n} runs per step",
+                       "inference": "tensor cores (mma.sync bf16)" if args.is_tc else "cuda cores (oracle order)",
+                       "kernel": "one thread per run" if family == 5 else "one warp per run",
                        "ce_rounds": len(log.rounds), "launches_before_timed": 2 * len(log.rounds) + args.warmup},
             "run_steps_per_s": steps / t, "steps_per_run": steps / (n * args.steps)}
     if rank == 0:
@@ -692,6 +731,20 @@ def main():
                          "smaller values are for profiling captures)")
     ap.add_argument("--is-eval-runs", type=int, default=0,
                     help="rare_is: also evaluate the trained proposal on this many weighted runs (e.g. 10000000)")
+    ap.add_argument("--ce-rounds", type=int, default=0,
+                    help="rare_is: exactly this many CE rounds (default: IS_CE, stopping once settled)")
+    ap.add_argument("--ce-runs", type=int, default=0, help="rare_is: runs per CE round (default: IS_CE)")
+    ap.add_argument("--ce-steps", type=int, default=0, help="rare_is: Adam steps per CE round (default: IS_CE)")
+    ap.add_argument("--is-warp", action="store_true",
+                    help="rare_is / is_kernel: runs under the proposal one warp per run (the thread-per-run "
+                         "kernel is the default where the network qualifies)")
+    ap.add_argument("--is-tc", action="store_true",
+                    help="rare_is / is_kernel: theta by warp-level tensor-core MMAs instead of the CUDA-core "
+                         "evaluation in the oracle's order")
+    ap.add_argument("--batch-group-comps", default="-1",
+                    help="batch_64: networks with at least this many components run one warp per run "
+                         "(0: none; -1, the default: the autotuner's choice); further comma-separated "
+                         "thresholds are each timed once more and reported under group_sweep")
     ap.add_argument("--batch-divisor", type=int, default=0,
                     help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
     ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "is_kernel", "mlp_grad"],

@@ -167,6 +167,9 @@ _SIGNATURES = {
     "csmc_batch_set_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     "csmc_batch_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_int32)]),
+    "csmc_batch_set_group_comps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "csmc_batch_group_comps": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.POINTER(ctypes.c_int32)]),
     "csmc_batch_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "csmc_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Result)]),
     "csmc_batch_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Result)]),
@@ -179,6 +182,8 @@ _SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32)]),
     "csmc_batch_free": (None, [ctypes.c_void_p]),
     "csmc_is_set_inference": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "csmc_is_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "csmc_is_set_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     "csmc_is_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Query), ctypes.c_char_p, ctypes.c_uint64,
                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Result), ctypes.c_void_p]),

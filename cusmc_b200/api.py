@@ -213,6 +213,17 @@ class Batch:
         check(lib().csmc_batch_plan(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def set_group_comps(self, min_comps: int) -> None:
+        """Networks of min_comps .. 512 components run one warp per run (0:
+        none)."""
+        check(lib().csmc_batch_set_group_comps(self._h, min_comps))
+
+    def group_comps(self) -> tuple[int, int]:
+        """(warp-per-run threshold, number of jobs it selects)."""
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().csmc_batch_group_comps(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def autotune(self, probe_fraction: float = 0.05) -> tuple[int, int]:
         a, b = ctypes.c_int32(), ctypes.c_int32()
         check(lib().csmc_batch_autotune(self._h, probe_fraction, ctypes.byref(a), ctypes.byref(b)))

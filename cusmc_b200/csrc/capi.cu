@@ -77,9 +77,10 @@ bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std:
             why = "lane-group plans use 32..256 threads per CTA";
             return false;
         }
-        // per-group run state: 48 bytes of scalars, the variables, then one
-        // inverse rate per rate program (evaluated once per step)
-        const uint32_t stride = static_cast<uint32_t>((48 + 4 * (h.n_vars + h.n_rate_prog) + 15) & ~15u);
+        // per-group run state: 48 bytes of scalars, the variables, one
+        // inverse rate per rate program (evaluated once per step), the slot
+        // masks
+        const uint32_t stride = csmc::group_state_stride(h.n_vars, h.n_rate_prog, lanes, cpl);
         const size_t smem = n->bytes + static_cast<size_t>(block / lanes) * stride;
         if (smem > max_smem) {
             why = "network and run state do not fit in shared memory";
@@ -99,11 +100,14 @@ bool configure_plan(csmc_net *n, int family, int lanes, int cpl, int block, std:
         return false;
     }
     if (family == 4) {  // class-coded thread per run (sim_coded.cuh)
-        if (!n->classes || h.n_comps > 256 || h.max_locs_per_comp > 32) {
-            why = "the class-coded plan needs race classes, at most 256 components and 32 locations per automaton";
+        if (!n->classes || h.n_comps < 4 || h.n_comps > 256 || h.max_locs_per_comp > 32) {
+            why = "the class-coded plan needs race classes, 4 to 256 components and at most 32 locations per "
+                  "automaton";
             return false;
         }
-        const size_t slab = csmc::coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, n->slots, block);
+        const csmc::NetLayout L = csmc::layout_of(h);
+        const size_t slab = csmc::coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, n->slots, block, L.n_classes,
+                                                   (h.recv_chan_lo | h.recv_chan_hi) != 0);
         if (n->bytes + slab > max_smem) {
             why = "network and run state do not fit in shared memory";
             return false;
@@ -230,9 +234,10 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     p.scratch = n->d_scratch;
     int ctas = 0;
     p.keys = csmc::philox_keys(seed);
+    for (int g = 0; g < CSMC_RACE_CLASSES; ++g) p.class_src[g] = n->class_src[g];
     int rc = n->family == 0 ? csmc::sim_max_active_ctas(n->lanes, n->comps_per_lane, verify, n->block, n->smem, &ctas)
-             : n->family == 2 ? csmc::batch_max_active_ctas(verify, n->block, n->smem, &ctas)
-             : n->family == 4 ? csmc::coded_max_active_ctas(verify, n->slots, n->block, n->smem, &ctas)
+             : n->family == 2 ? csmc::batch_max_active_ctas(verify, 0, n->block, n->smem, &ctas)
+             : n->family == 4 ? csmc::coded_max_active_ctas(verify, n->slots, n->all_classed, n->block, n->smem, &ctas)
                               : csmc::serial_max_active_ctas(verify, n->slots, n->loc8, n->state_in_global, n->classes,
                                                              n->block, n->smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
@@ -294,7 +299,8 @@ int run_impl(const csmc_net *cn, const csmc_query *q, uint64_t seed, uint64_t fi
     rc = n->family == 0   ? csmc::sim_launch(n->lanes, n->comps_per_lane, verify, p, static_cast<int>(grid), n->block,
                                              n->smem, st)
          : n->family == 2 ? csmc::batch_launch(verify, bp, static_cast<int>(grid), n->block, st)
-         : n->family == 4 ? csmc::coded_launch(verify, n->slots, p, static_cast<int>(grid), n->block, n->smem, st)
+         : n->family == 4 ? csmc::coded_launch(verify, n->slots, n->all_classed, p, static_cast<int>(grid), n->block,
+                                               n->smem, st)
                           : csmc::serial_launch(verify, n->slots, n->loc8, n->state_in_global, n->classes, p,
                                                 static_cast<int>(grid), n->block, n->smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "simulation kernel launch");
@@ -447,6 +453,56 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
     n->slots = h->max_edges_per_loc >= 2;
     n->loc8 = h->max_locs_per_comp <= 256;
     n->classes = (h->flags & CSMC_NET_RACE_CLASSES) != 0 && h->n_comps <= 256;
+    if (n->classes && h->off_loc_desc + 8ull * h->n_locs > h->total_bytes)
+        return fail(CSMC_ERR_ARG, "not a network blob (descriptor table out of range)");
+    if (n->classes) {
+        // each class's 1/rate source, and whether every location is classed
+        // (the class-coded kernel's launch parameters)
+        const uint8_t *base = static_cast<const uint8_t *>(blob);
+        n->all_classed = true;
+        for (uint32_t i = 0; i < h->n_locs; ++i) {
+            uint64_t d;
+            std::memcpy(&d, base + h->off_loc_desc + 8ull * i, 8);
+            const uint32_t lo = static_cast<uint32_t>(d), fl = static_cast<uint32_t>(d >> 32);
+            const uint32_t g = CSMC_DESC_CLASS(fl);
+            if (g >= CSMC_RACE_CLASSES) {
+                n->all_classed = false;
+                continue;
+            }
+            n->class_src[g] = (fl & CSMC_DESC_PROG) ? (CSMC_CLASS_SRC_PROG | lo) : lo;
+        }
+        // tilt groups of importance sampling one thread per run: the
+        // (race class, location class) pairs in order of first appearance,
+        // the first CSMC_IS_GROUPS of them; later pairs take the
+        // descriptor path (code 7)
+        if (h->n_comps >= 4 && h->max_locs_per_comp <= 32 && h->off_comp + 8ull * h->n_comps <= h->total_bytes) {
+            int8_t id[CSMC_RACE_CLASSES][4];
+            std::memset(id, -1, sizeof id);
+            int groups = 0;
+            uint64_t map = 0;
+            for (uint32_t c = 0; c < h->n_comps; ++c) {
+                csmc_comp cp;
+                std::memcpy(&cp, base + h->off_comp + 8ull * c, sizeof cp);
+                for (uint32_t k = 0; k < cp.n_locs && cp.loc_begin + k < h->n_locs; ++k) {
+                    uint64_t d;
+                    std::memcpy(&d, base + h->off_loc_desc + 8ull * (cp.loc_begin + k), 8);
+                    const uint32_t g = CSMC_DESC_CLASS(static_cast<uint32_t>(d >> 32));
+                    if (g >= CSMC_RACE_CLASSES || id[g][k & 3u] >= 0) continue;
+                    id[g][k & 3u] = static_cast<int8_t>(groups < CSMC_IS_GROUPS ? groups : 7);
+                    if (groups < CSMC_IS_GROUPS) {
+                        n->is_group_src[groups] = n->class_src[g];
+                        n->is_group_l |= (k & 3u) << (2 * groups);
+                        ++groups;
+                    }
+                }
+            }
+            for (uint32_t g = 0; g < CSMC_RACE_CLASSES; ++g)
+                for (uint32_t l = 0; l < 4; ++l)
+                    map |= static_cast<uint64_t>(id[g][l] < 0 ? 7 : id[g][l]) << (3 * (4 * g + l));
+            n->is_group_map = map;
+            n->is_groups = groups;
+        }
+    }
     // default plan: the class-coded thread-per-run kernel when the network
     // has race classes and fits its limits; else one thread per run when the
     // run state of a 128-thread CTA fits next to the network in shared

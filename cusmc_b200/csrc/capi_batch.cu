@@ -15,6 +15,12 @@
 #include <string>
 #include <vector>
 
+// Jobs whose networks have at least this many components (and at most
+// CSMC_BATCH_GROUP_MAX_COMPS) run one warp per run by default.
+constexpr uint32_t kDefaultGroupMinComps = 128;
+// Counter words before the per-job counters: the two run queues.
+constexpr size_t kQueueWords = 2;
+
 struct csmc_batch {
     int device = 0;
     int n_jobs = 0;
@@ -23,19 +29,24 @@ struct csmc_batch {
     std::vector<csmc_query> qs;
     std::vector<uint64_t> seeds, first_runs, n_runs;
     std::vector<double> cost;          // estimated device cost of one run, per job
-    std::vector<int> order;            // run-space position -> job
+    std::vector<int> order;            // job-table position -> job: warp-per-run jobs first, each part by cost
+    std::vector<char> group;           // per job: simulated one warp per run
+    int n_group = 0;                   // warp-per-run jobs
+    uint32_t group_min_comps = kDefaultGroupMinComps;  // networks this large run one warp per run (0: none do)
+    int group_k = 0;                   // components per lane of the warp-per-run jobs
+    uint32_t group_stride = 0;         // shared memory of one warp-per-run run state
     std::vector<uint64_t> out_off;     // per job: first run's index in the output buffers
     std::vector<uint64_t> fs_off;      // per job: offset of its final states (words)
     uint64_t total_runs = 0;
-    uint32_t max_v = 0, max_p = 0, max_c = 0;
-    csmc::BatchJob *d_jobs = nullptr;  // in run-space order
+    uint32_t max_v = 0, max_p = 0, max_c = 0;  // over the thread-per-run jobs
+    csmc::BatchJob *d_jobs = nullptr;  // in job-table order
     uint8_t *d_flags = nullptr;
     double *d_values = nullptr;
     uint32_t *d_steps = nullptr;
     uint64_t *d_digests = nullptr;
     uint32_t *d_final = nullptr;
-    unsigned long long *d_counters = nullptr;  // [0] queue, then 4 words per run-space position
-    double *d_partials = nullptr;              // 2 * kReduceBlocks per run-space position
+    unsigned long long *d_counters = nullptr;  // [0] thread-per-run queue, [1] warp-per-run queue, then 4 words per job-table position
+    double *d_partials = nullptr;              // 2 * kReduceBlocks per job-table position
     unsigned long long *h_counters = nullptr;  // pinned copies
     double *h_partials = nullptr;
     uint8_t *d_state = nullptr;
@@ -84,11 +95,51 @@ void drop_graph(csmc_batch *b) {
     b->exec = nullptr;
 }
 
-// Job table in run-space order for the given per-job run counts; step_cap
-// (0: none) limits every run's race steps (autotuner probes).
+// Which jobs run one warp per run (networks of group_min_comps ..
+// CSMC_BATCH_GROUP_MAX_COMPS components), the job-table order (those jobs
+// first, each part by falling cost), the lanes' component count and the
+// state sizes of both parts.
+void assign_modes(csmc_batch *b) {
+    b->group.assign(b->n_jobs, 0);
+    b->n_group = 0;
+    b->max_v = b->max_p = b->max_c = 0;
+    uint32_t gmax_c = 0, gmax_vp = 0;
+    for (int j = 0; j < b->n_jobs; ++j) {
+        const csmc_net_header &h = b->nets[j]->h;
+        const bool g = b->group_min_comps > 0 && h.n_comps >= b->group_min_comps &&
+                       h.n_comps <= CSMC_BATCH_GROUP_MAX_COMPS;
+        b->group[j] = g;
+        if (g) {
+            ++b->n_group;
+            gmax_c = std::max(gmax_c, h.n_comps);
+            gmax_vp = std::max(gmax_vp, h.n_vars + h.n_rate_prog);
+        } else {
+            b->max_v = std::max(b->max_v, h.n_vars);
+            b->max_p = std::max(b->max_p, h.n_rate_prog);
+            b->max_c = std::max(b->max_c, h.n_comps);
+        }
+    }
+    b->group_k = gmax_c == 0 ? 0 : gmax_c <= 128 ? 4 : gmax_c <= 256 ? 8 : 16;
+    b->group_stride = b->n_group ? csmc::group_state_stride(gmax_vp, 0, 32, b->group_k) : 0;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+        if (b->group[x] != b->group[y]) return b->group[x] > b->group[y];
+        return b->cost[x] > b->cost[y];
+    });
+}
+
+// Runs of the thread-per-run part and of the warp-per-run part.
+void part_totals(const csmc_batch *b, const std::vector<uint64_t> &runs, uint64_t *thread_runs,
+                 uint64_t *group_runs) {
+    *thread_runs = *group_runs = 0;
+    for (int j = 0; j < b->n_jobs; ++j) (b->group[j] ? *group_runs : *thread_runs) += runs[j];
+}
+
+// Job table in job-table order for the given per-job run counts (each part
+// numbers its runs from 0); step_cap (0: none) limits every run's race
+// steps (autotuner probes).
 std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<uint64_t> &runs, uint64_t step_cap = 0) {
     std::vector<csmc::BatchJob> t(b->n_jobs);
-    uint64_t begin = 0;
+    uint64_t begin[2] = {0, 0};
     for (int k = 0; k < b->n_jobs; ++k) {
         const int j = b->order[k];
         const csmc_net *n = b->nets[j];
@@ -97,7 +148,7 @@ std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<u
         std::memset(&J, 0, sizeof J);
         J.net = csmc::layout_of(n->h);
         J.blob = n->d_blob;
-        J.run_begin = begin;
+        J.run_begin = begin[b->group[j] ? 1 : 0];
         J.n_runs = runs[j];
         J.first_run = b->first_runs[j];
         J.seed = b->seeds[j];
@@ -113,8 +164,8 @@ std::vector<csmc::BatchJob> build_table(const csmc_batch *b, const std::vector<u
         J.steps = b->d_steps + b->out_off[j];
         J.digests = b->d_digests ? b->d_digests + b->out_off[j] : nullptr;
         J.final_state = b->d_final ? b->d_final + b->fs_off[j] : nullptr;
-        J.counters = b->d_counters + 1 + 4 * static_cast<size_t>(k);
-        begin += runs[j];
+        J.counters = b->d_counters + kQueueWords + 4 * static_cast<size_t>(k);
+        begin[b->group[j] ? 1 : 0] += runs[j];
     }
     return t;
 }
@@ -126,21 +177,28 @@ int upload_table(csmc_batch *b, const std::vector<uint64_t> &runs, uint64_t step
     return CSMC_OK;
 }
 
+size_t launch_smem(const csmc_batch *b, int block) {
+    return csmc::batch_smem_bytes(b->n_jobs, b->n_group ? b->group_stride : 0u, block);
+}
+
 // Grid and state slabs for the current geometry.
 int configure(csmc_batch *b) {
     int ctas = 0, sms = 0;
-    const size_t smem = csmc::batch_smem_bytes(b->n_jobs);
-    int rc = csmc::batch_max_active_ctas(b->verify, b->block, smem, &ctas);
+    const size_t smem = launch_smem(b, b->block);
+    int rc = csmc::batch_max_active_ctas(b->verify, b->n_group ? b->group_k : 0, b->block, smem, &ctas);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
     if (ctas < 1) return fail(CSMC_ERR_LIMIT, "batch kernel cannot be resident");
     if (b->ctas_per_sm > 0) ctas = std::min(ctas, b->ctas_per_sm);
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "cudaDeviceGetAttribute");
     uint64_t grid = static_cast<uint64_t>(sms) * ctas;
-    const uint64_t needed = (b->total_runs + b->block - 1) / b->block;
+    uint64_t thread_runs = 0, group_runs = 0;
+    part_totals(b, b->n_runs, &thread_runs, &group_runs);
+    const uint64_t warps = b->block / 32;
+    const uint64_t needed = (thread_runs + b->block - 1) / b->block + (group_runs + warps - 1) / warps;
     grid = std::max<uint64_t>(1, std::min(grid, needed));
-    const size_t per = csmc::batch_state_bytes_per_thread(b->max_c, b->max_v, b->max_p);
+    const size_t per = b->n_group == b->n_jobs ? 0 : csmc::batch_state_bytes_per_thread(b->max_c, b->max_v, b->max_p);
     b->state_stride = static_cast<uint32_t>((per * b->block + 15) & ~static_cast<size_t>(15));
-    const size_t need = grid * static_cast<size_t>(b->state_stride);
+    const size_t need = std::max<size_t>(16, grid * static_cast<size_t>(b->state_stride));
     if (need > b->state_bytes) {
         cudaFree(b->d_state);
         b->d_state = nullptr;
@@ -154,25 +212,31 @@ int configure(csmc_batch *b) {
 }
 
 // The launch sequence: no allocation, no synchronisation (capturable).
-int launch_impl(csmc_batch *b, cudaStream_t st, uint64_t total_runs) {
-    CK(cudaMemsetAsync(b->d_counters, 0, (1 + 4 * static_cast<size_t>(b->n_jobs)) * sizeof(unsigned long long), st),
-       "cudaMemsetAsync(batch counters)");
+int launch_impl(csmc_batch *b, cudaStream_t st, const std::vector<uint64_t> &runs) {
+    const size_t words = kQueueWords + 4 * static_cast<size_t>(b->n_jobs);
+    CK(cudaMemsetAsync(b->d_counters, 0, words * sizeof(unsigned long long), st), "cudaMemsetAsync(batch counters)");
+    uint64_t thread_runs = 0, group_runs = 0;
+    part_totals(b, runs, &thread_runs, &group_runs);
     csmc::BatchParams p{};
     p.jobs = b->d_jobs;
     p.n_jobs = static_cast<uint32_t>(b->n_jobs);
     p.state_stride = b->state_stride;
-    p.total_runs = total_runs;
+    p.total_runs = thread_runs;
     p.queue = b->d_counters;
     p.state = b->d_state;
     p.max_vars = b->max_v;
     p.max_rate_prog = b->max_p;
     p.max_comps = b->max_c;
+    p.n_group_jobs = static_cast<uint32_t>(b->n_group);
+    p.group_runs = group_runs;
+    p.group_queue = b->n_group ? b->d_counters + 1 : nullptr;
+    p.group_stride = b->group_stride;
+    p.group_k = static_cast<uint32_t>(b->group_k);
     int rc = csmc::batch_launch(b->verify, p, b->grid, b->block, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "batch kernel launch");
     reduce_jobs<<<dim3(csmc::kReduceBlocks, b->n_jobs), 256, 0, st>>>(b->d_jobs, b->d_partials);
     CK(cudaGetLastError(), "reduce launch");
-    CK(cudaMemcpyAsync(b->h_counters, b->d_counters, (1 + 4 * static_cast<size_t>(b->n_jobs)) * sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, st),
+    CK(cudaMemcpyAsync(b->h_counters, b->d_counters, words * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
        "cudaMemcpyAsync(batch counters)");
     CK(cudaMemcpyAsync(b->h_partials, b->d_partials,
                        2 * csmc::kReduceBlocks * static_cast<size_t>(b->n_jobs) * sizeof(double), cudaMemcpyDeviceToHost,
@@ -186,10 +250,11 @@ void fill_results(const csmc_batch *b, const std::vector<uint64_t> &runs, float 
         const int j = b->order[k];
         csmc_result &r = outs[j];
         std::memset(&r, 0, sizeof r);
+        const unsigned long long *c = b->h_counters + kQueueWords + 4 * static_cast<size_t>(k);
         r.runs = runs[j];
-        r.hits = b->h_counters[1 + 4 * k];
-        r.steps = b->h_counters[2 + 4 * k];
-        r.capped = b->h_counters[3 + 4 * k];
+        r.hits = c[0];
+        r.steps = c[1];
+        r.capped = c[2];
         const double *part = b->h_partials + static_cast<size_t>(k) * 2 * csmc::kReduceBlocks;
         for (int i = 0; i < csmc::kReduceBlocks; ++i) {
             r.sum += part[2 * i];
@@ -200,9 +265,9 @@ void fill_results(const csmc_batch *b, const std::vector<uint64_t> &runs, float 
         else if (q.kind == CSMC_QUERY_VARIABLE && q.is_estimate) r.estimate = r.sum / static_cast<double>(r.runs);
         else r.estimate = static_cast<double>(r.hits) / static_cast<double>(r.runs);
         r.kernel_ms = ms;
-        r.lanes_per_run = 1;
-        r.comps_per_lane = static_cast<int32_t>(b->nets[j]->h.n_comps);
-        r.runs_per_cta = b->block;
+        r.lanes_per_run = b->group[j] ? 32 : 1;
+        r.comps_per_lane = b->group[j] ? b->group_k : static_cast<int32_t>(b->nets[j]->h.n_comps);
+        r.runs_per_cta = b->group[j] ? b->block / 32 : b->block;
         r.family = 2;
     }
 }
@@ -216,18 +281,19 @@ constexpr uint64_t kProbeSteps = 2000;
 int probe(csmc_batch *b, const std::vector<uint64_t> &runs, float *ms, std::vector<uint64_t> *steps_out) {
     int rc = upload_table(b, runs, kProbeSteps);
     if (rc) return rc;
-    const uint64_t total = std::accumulate(runs.begin(), runs.end(), uint64_t{0});
     cudaStream_t st = nullptr;
     CK(cudaEventRecord(b->ev0, st), "cudaEventRecord");
-    rc = launch_impl(b, st, total);
+    rc = launch_impl(b, st, runs);
     if (rc) return rc;
     CK(cudaEventRecord(b->ev1, st), "cudaEventRecord");
     CK(cudaStreamSynchronize(st), "batch probe");
     CK(cudaEventElapsedTime(ms, b->ev0, b->ev1), "cudaEventElapsedTime");
     if (steps_out) {  // per job: steps, or 0 when some run hit the probe's cap
         steps_out->assign(b->n_jobs, 0);
-        for (int k = 0; k < b->n_jobs; ++k)
-            (*steps_out)[b->order[k]] = b->h_counters[3 + 4 * k] ? 0 : b->h_counters[2 + 4 * k];
+        for (int k = 0; k < b->n_jobs; ++k) {
+            const unsigned long long *c = b->h_counters + kQueueWords + 4 * static_cast<size_t>(k);
+            (*steps_out)[b->order[k]] = c[2] ? 0 : c[1];
+        }
     }
     return CSMC_OK;
 }
@@ -265,15 +331,12 @@ int csmc_batch_create(csmc_net *const *nets, const csmc_query *qs, const uint64_
         b->fs_off.push_back(fs_words);
         b->total_runs += n_runs[j];
         fs_words += n_runs[j] * (n->h.n_comps + n->h.n_vars);
-        b->max_v = std::max(b->max_v, n->h.n_vars);
-        b->max_p = std::max(b->max_p, n->h.n_rate_prog);
-        b->max_c = std::max(b->max_c, n->h.n_comps);
         // until measured: cost of a run ~ components x horizon
         b->cost.push_back(static_cast<double>(n->h.n_comps) * std::max(1.0, qs[j].horizon));
     }
     b->order.resize(n_jobs);
     std::iota(b->order.begin(), b->order.end(), 0);
-    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->cost[x] > b->cost[y]; });
+    assign_modes(b.get());
     const uint64_t R = std::max<uint64_t>(b->total_runs, 1);
     CK(cudaMalloc(&b->d_jobs, n_jobs * sizeof(csmc::BatchJob)), "cudaMalloc(job table)");
     CK(cudaMalloc(&b->d_flags, R), "cudaMalloc(flags)");
@@ -283,7 +346,7 @@ int csmc_batch_create(csmc_net *const *nets, const csmc_query *qs, const uint64_
         CK(cudaMalloc(&b->d_digests, R * sizeof(uint64_t)), "cudaMalloc(digests)");
         CK(cudaMalloc(&b->d_final, std::max<uint64_t>(fs_words, 1) * sizeof(uint32_t)), "cudaMalloc(final states)");
     }
-    const size_t counters = 1 + 4 * static_cast<size_t>(n_jobs);
+    const size_t counters = kQueueWords + 4 * static_cast<size_t>(n_jobs);
     const size_t partials = 2 * csmc::kReduceBlocks * static_cast<size_t>(n_jobs);
     CK(cudaMalloc(&b->d_counters, counters * sizeof(unsigned long long)), "cudaMalloc(counters)");
     CK(cudaMalloc(&b->d_partials, partials * sizeof(double)), "cudaMalloc(partials)");
@@ -322,7 +385,25 @@ int csmc_batch_plan(const csmc_batch *b, int32_t *threads_per_cta, int32_t *ctas
 
 int csmc_batch_launch(csmc_batch *b, void *stream) {
     if (!b) return fail(CSMC_ERR_ARG, "null argument");
-    return launch_impl(b, static_cast<cudaStream_t>(stream), b->total_runs);
+    return launch_impl(b, static_cast<cudaStream_t>(stream), b->n_runs);
+}
+
+int csmc_batch_set_group_comps(csmc_batch *b, int32_t min_comps) {
+    if (!b) return fail(CSMC_ERR_ARG, "null argument");
+    if (min_comps < 0) return fail(CSMC_ERR_ARG, "negative component threshold");
+    CK(cudaSetDevice(b->device), "cudaSetDevice");
+    b->group_min_comps = static_cast<uint32_t>(min_comps);
+    assign_modes(b);
+    int rc = configure(b);
+    if (rc) return rc;
+    return upload_table(b, b->n_runs);
+}
+
+int csmc_batch_group_comps(const csmc_batch *b, int32_t *min_comps, int32_t *group_jobs) {
+    if (!b) return fail(CSMC_ERR_ARG, "null argument");
+    if (min_comps) *min_comps = static_cast<int32_t>(b->group_min_comps);
+    if (group_jobs) *group_jobs = b->n_group;
+    return CSMC_OK;
 }
 
 int csmc_batch_results(const csmc_batch *b, csmc_result *outs) {
@@ -338,7 +419,7 @@ int csmc_batch_run(csmc_batch *b, int32_t use_graph, void *stream, csmc_result *
     if (use_graph && !b->exec) {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-        int rc = launch_impl(b, b->cap, b->total_runs);
+        int rc = launch_impl(b, b->cap, b->n_runs);
         cudaError_t e = cudaStreamEndCapture(b->cap, &g);
         if (rc) {
             if (g) cudaGraphDestroy(g);
@@ -356,7 +437,7 @@ int csmc_batch_run(csmc_batch *b, int32_t use_graph, void *stream, csmc_result *
     if (use_graph) {
         CK(cudaGraphLaunch(b->exec, st), "cudaGraphLaunch");
     } else {
-        int rc = launch_impl(b, st, b->total_runs);
+        int rc = launch_impl(b, st, b->n_runs);
         if (rc) return rc;
     }
     CK(cudaEventRecord(b->ev1, st), "cudaEventRecord");
@@ -419,13 +500,13 @@ int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_p
     for (int j = 0; j < b->n_jobs; ++j)  // measured cost per run where no probe run was capped
         if (runs[j] && steps[j])
             b->cost[j] = static_cast<double>(steps[j]) / runs[j] * std::max<uint32_t>(1, b->nets[j]->h.n_comps);
-    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->cost[x] > b->cost[y]; });
+    assign_modes(b);
     // 2. geometry: threads per CTA x CTAs per SM
     int best_block = save_block, best_ctas = save_ctas;
     float best_ms = -1.0f;
     for (int block : {64, 128}) {
         int maxc = 0;
-        rc = csmc::batch_max_active_ctas(b->verify, block, csmc::batch_smem_bytes(b->n_jobs), &maxc);
+        rc = csmc::batch_max_active_ctas(b->verify, b->n_group ? b->group_k : 0, block, launch_smem(b, block), &maxc);
         if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "occupancy query");
         for (int c = maxc; c >= 1 && c >= maxc - 3; --c) {
             b->block = block;
@@ -443,6 +524,24 @@ int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_p
     }
     b->block = best_block;
     b->ctas_per_sm = best_ctas;
+    // 3. which networks run one warp per run, at that geometry
+    const uint32_t save_min = b->group_min_comps;
+    uint32_t best_min = save_min;
+    for (uint32_t m : {0u, 64u, 128u, 256u}) {
+        if (m == save_min) continue;
+        b->group_min_comps = m;
+        assign_modes(b);
+        rc = configure(b);
+        if (rc) return rc;
+        rc = probe(b, runs, &ms, nullptr);
+        if (rc) return rc;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_min = m;
+        }
+    }
+    b->group_min_comps = best_min;
+    assign_modes(b);
     rc = configure(b);
     if (rc) return rc;
     rc = upload_table(b, b->n_runs);

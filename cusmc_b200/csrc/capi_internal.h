@@ -31,6 +31,8 @@ struct csmc_net {
     bool slots = false;
     bool loc8 = false;     // every automaton has at most 256 locations
     bool classes = false;  // delay descriptors carry race classes
+    bool all_classed = false;  // every location belongs to a race class
+    uint32_t class_src[CSMC_RACE_CLASSES] = {};  // 1/rate source of each class (SimParams::class_src)
     bool state_in_global = false;
     uint8_t *d_state = nullptr;  // thread-per-run state slabs (global-state plans)
     size_t state_bytes = 0;
@@ -41,6 +43,15 @@ struct csmc_net {
     uint8_t *d_is_flags = nullptr;
     uint64_t is_cap = 0;
     bool is_tc = false;  // importance sampling: theta by warp-level MMAs (false: the oracle-identical CUDA-core evaluation)
+    bool is_feat_set = false;   // importance sampling: a feature source was chosen (else the default)
+    csmc::MlpFeatures is_feat{};
+    // importance sampling one thread per run (sim_is_coded.cuh): the tilt
+    // groups of the network (is_groups < 0: the network does not qualify)
+    int is_groups = -1;
+    uint64_t is_group_map = 0;
+    uint32_t is_group_l = 0;
+    uint32_t is_group_src[CSMC_IS_GROUPS] = {};
+    int is_kernel = 0;  // 0: thread per run where the network qualifies, 3: always one warp per run
 };
 
 namespace csmc {

@@ -89,6 +89,40 @@ int plan_is(const csmc_net *n, bool trace, uint64_t n_runs, Launch &L) {
     return CSMC_OK;
 }
 
+// One thread per run (sim_is_coded.cuh) where the network has tilt groups,
+// theta is evaluated on CUDA cores and the CTA's state fits; false: the
+// one-warp-per-run kernel runs.
+bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
+    if (n->is_kernel == 3 || n->is_tc || n->is_groups < 0) return false;
+    const csmc_net_header &h = n->h;
+    L.slots = h.max_edges_per_loc >= 2;
+    L.loc8 = true;
+    int max_smem = 0, sms = 0, ctas = 0;
+    if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device) != cudaSuccess)
+        return false;
+    // a launch of few runs (a CE round) is bound by the steps of single
+    // runs: smaller CTAs spread its warps over more SMs
+    L.block = 128;
+    while (L.block > 32 && n_runs < 2ull * sms * L.block) L.block /= 2;
+    const bool recv = (h.recv_chan_lo | h.recv_chan_hi) != 0;
+    const size_t slab = csmc::is_coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, L.block,
+                                                  static_cast<uint32_t>(n->is_groups), recv);
+    L.smem = n->bytes + csmc::is_coded_mlp_smem_bytes() + (L.block / 32) * (4u * CSMC_MLP_HID * CSMC_MLP_CLASSES) +
+             slab;
+    if (L.smem > static_cast<size_t>(max_smem)) return false;
+    if (csmc::is_coded_max_active_ctas(L.slots, L.block, L.smem, &ctas) != 0 || ctas < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    uint64_t grid = static_cast<uint64_t>(sms) * ctas;
+    const uint64_t needed = (n_runs + L.block - 1) / L.block;
+    if (grid > needed) grid = needed;
+    L.grid = static_cast<int>(grid);
+    L.slab = 0;
+    return true;
+}
+
 csmc::IsParams base_params(const csmc_net *n, const csmc_query *q, uint64_t seed, uint64_t first_run,
                            uint64_t n_runs) {
     csmc::IsParams ip{};
@@ -106,7 +140,13 @@ csmc::IsParams base_params(const csmc_net *n, const csmc_query *q, uint64_t seed
     p.first_run = first_run;
     p.n_runs = n_runs;
     p.scratch = n->d_scratch;
+    p.keys = csmc::philox_keys(seed);
     ip.mlp = n->d_mlp;
+    ip.feat = n->is_feat_set ? n->is_feat : csmc::mlp_default_features(n->h.n_vars, n->h.n_comps);
+    ip.n_groups = n->is_groups > 0 ? static_cast<uint32_t>(n->is_groups) : 0u;
+    ip.group_map = n->is_group_map;
+    ip.group_l = n->is_group_l;
+    for (int g = 0; g < CSMC_IS_GROUPS; ++g) ip.group_src[g] = n->is_group_src[g];
     return ip;
 }
 
@@ -124,6 +164,36 @@ extern "C" {
 int csmc_is_set_inference(csmc_net *n, int32_t tensor_cores) {
     if (!n) return fail(CSMC_ERR_ARG, "null argument");
     n->is_tc = tensor_cores != 0;
+    return CSMC_OK;
+}
+
+int csmc_is_set_kernel(csmc_net *n, int32_t family) {
+    if (!n) return fail(CSMC_ERR_ARG, "null argument");
+    if (family != 0 && family != 3) return fail(CSMC_ERR_ARG, "importance-sampling kernel family must be 0 or 3");
+    n->is_kernel = family;
+    return CSMC_OK;
+}
+
+int csmc_is_set_features(csmc_net *n, const int32_t *count_vars, const float *scales, int32_t clock_var) {
+    if (!n) return fail(CSMC_ERR_ARG, "null argument");
+    if (!count_vars && !scales && clock_var < 0) {
+        n->is_feat_set = false;
+        return CSMC_OK;
+    }
+    csmc::MlpFeatures F = csmc::mlp_default_features(n->h.n_vars, n->h.n_comps);
+    for (int i = 0; i < 4; ++i) {
+        if (count_vars) F.var[i] = count_vars[i] < 0 ? -1 : count_vars[i];
+        if (scales) F.scale[i] = scales[i];
+        if (F.var[i] >= 0 && static_cast<uint32_t>(F.var[i]) >= n->h.n_vars)
+            return fail(CSMC_ERR_ARG, "feature variable id " + std::to_string(F.var[i]) + " out of range");
+        if (!(F.scale[i] == F.scale[i]) || F.scale[i] > 3.0e38f || F.scale[i] < -3.0e38f)
+            return fail(CSMC_ERR_ARG, "feature scales must be finite");
+    }
+    if (clock_var >= 0 && static_cast<uint32_t>(clock_var) >= n->h.n_vars)
+        return fail(CSMC_ERR_ARG, "clock feature variable id out of range");
+    F.clock_var = clock_var < 0 ? -1 : clock_var;
+    n->is_feat = F;
+    n->is_feat_set = true;
     return CSMC_OK;
 }
 
@@ -146,12 +216,20 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
     rc = ensure_is_buffers(n, n_runs);
     if (rc) return rc;
     Launch L;
-    rc = plan_is(n, false, n_runs, L);
-    if (rc) return rc;
+    const bool coded = plan_is_coded(n, n_runs, L);
+    if (!coded) {
+        rc = plan_is(n, false, n_runs, L);
+        if (rc) return rc;
+    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     CK(cudaMemcpyAsync(n->d_mlp, params, sizeof(csmc::MlpParams), cudaMemcpyHostToDevice, st), "upload proposal");
     CK(cudaMemsetAsync(n->d_scratch, 0, CSMC_SCRATCH_WORDS * sizeof(unsigned long long), st), "cudaMemsetAsync");
-    out->runs_per_cta = L.block / 32;
+    out->runs_per_cta = coded ? L.block : L.block / 32;
+    if (coded) {
+        out->lanes_per_run = 1;
+        out->comps_per_lane = static_cast<int32_t>(n->h.n_comps);
+        out->family = 5;
+    }
     csmc::IsParams ip = base_params(n, q, seed, first_run, n_runs);
     ip.slab_bytes = L.slab;
     ip.s.flags = flags ? flags : n->d_is_flags;
@@ -160,7 +238,8 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
     ip.logw = logw;
     ip.wvals = n->d_wvals;
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
-    rc = csmc::is_launch(n->is_tc, false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
+    rc = coded ? csmc::is_coded_launch(L.slots, ip, L.grid, L.block, L.smem, st)
+               : csmc::is_launch(n->is_tc, false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "importance-sampling kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");
     reduce_weights<<<csmc::kReduceBlocks, 256, 0, st>>>(n->d_wvals, n_runs, n->d_partials);

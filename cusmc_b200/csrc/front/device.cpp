@@ -700,11 +700,20 @@ class Packer {
             if (!reads_clock) h.flags |= CSMC_NET_RATE_NO_CLOCK;
         }
         std::vector<uint64_t> loc_desc;
+        std::vector<uint32_t> loc_inv1(locs_.size(), 0u);
         for (size_t i = 0; i < locs_.size(); ++i) {
             const csmc_loc &pl = locs_[i];
             uint32_t flags = 0, lo = 0;
             if (pl.type > 1) flags |= CSMC_DESC_ZERO;
             if (pl.n_inv) flags |= CSMC_DESC_INV;
+            if (pl.n_inv == 1) {  // one clock bound by a literal: inline in the kernels
+                const csmc_guard &g = guards_[pl.inv_begin];
+                const uint32_t k = CSMC_H_PAYLOAD(g.rhs);
+                if (CSMC_H_TAG(g.rhs) == CSMC_H_LIT && k < 0x8000u && g.var <= 0xffffu) {
+                    flags |= CSMC_DESC_INV1;
+                    loc_inv1[i] = (static_cast<uint32_t>(g.var) << 16) | ((g.op == CSMC_G_LT ? 1u : 0u) << 15) | k;
+                }
+            }
             const uint16_t slot = loc_rate[i];
             if (slot & CSMC_RATE_PROG_BIT) {
                 if (h.flags & CSMC_NET_RATE_TABLE) {
@@ -716,30 +725,55 @@ class Packer {
             } else {
                 std::memcpy(&lo, &inv_lit[slot], 4);
             }
+            if (flags & CSMC_DESC_EVAL) {  // the inline invariant path reads the rate from the descriptor
+                flags &= ~CSMC_DESC_INV1;
+                loc_inv1[i] = 0u;
+            }
             loc_desc.push_back(static_cast<uint64_t>(lo) | (static_cast<uint64_t>(flags) << 32));
         }
         // race classes: always-exponential locations sharing the source of
         // their 1/rate (a literal of finite positive value, or one per-step
-        // rate program)
+        // rate program) of at least two locations.  With more than
+        // CSMC_RACE_CLASSES such sources, the ones with the most locations
+        // get classes (ids in order of first appearance) and the other
+        // locations race through their descriptor.
         {
-            std::map<uint64_t, uint32_t> cls;
-            bool ok = comps_.size() <= 256;
-            for (uint64_t &d : loc_desc) {
+            auto class_key = [](uint64_t d, uint64_t &key) {
                 const uint32_t fl = static_cast<uint32_t>(d >> 32), lo = static_cast<uint32_t>(d);
                 float inv;
                 std::memcpy(&inv, &lo, 4);
                 const bool lit_ok = (fl & CSMC_DESC_PROG) || (inv > 0.0f && inv <= std::numeric_limits<float>::max());
+                key = d & (0xffffffffull | (static_cast<uint64_t>(CSMC_DESC_PROG) << 32));
+                return !(fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL)) && lit_ok;
+            };
+            std::vector<uint64_t> order;  // keys in order of first appearance
+            std::map<uint64_t, uint32_t> count;
+            for (uint64_t d : loc_desc) {
+                uint64_t key;
+                if (!class_key(d, key)) continue;
+                if (!count[key]++) order.push_back(key);
+            }
+            // a source shared by a single location gains nothing from a class
+            std::vector<uint64_t> ranked;
+            for (uint64_t key : order)
+                if (count[key] >= 2) ranked.push_back(key);
+            std::stable_sort(ranked.begin(), ranked.end(),
+                             [&](uint64_t a, uint64_t b) { return count[a] > count[b]; });
+            if (ranked.size() > CSMC_RACE_CLASSES) ranked.resize(CSMC_RACE_CLASSES);
+            std::map<uint64_t, uint32_t> cls;
+            for (uint64_t key : order)
+                if (std::find(ranked.begin(), ranked.end(), key) != ranked.end())
+                    cls.emplace(key, static_cast<uint32_t>(cls.size()));
+            for (uint64_t &d : loc_desc) {
+                uint64_t key;
                 uint32_t c = CSMC_DESC_NO_CLASS;
-                if (!(fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL)) && lit_ok) {
-                    const uint64_t key = d & (0xffffffffull | (static_cast<uint64_t>(CSMC_DESC_PROG) << 32));
+                if (class_key(d, key)) {
                     auto it = cls.find(key);
-                    if (it == cls.end()) it = cls.emplace(key, static_cast<uint32_t>(cls.size())).first;
-                    if (it->second >= CSMC_RACE_CLASSES) ok = false;
-                    c = it->second & 0xffu;
+                    if (it != cls.end()) c = it->second;
                 }
                 d |= static_cast<uint64_t>(c << 8) << 32;
             }
-            if (ok && !cls.empty()) {
+            if (comps_.size() <= 256 && !cls.empty()) {
                 h.flags |= CSMC_NET_RACE_CLASSES;
                 h.n_classes = static_cast<uint32_t>(cls.size());
             }
@@ -776,6 +810,7 @@ class Packer {
         h.off_rate_prog = section(rate_prog.data(), rate_prog.size() * sizeof(uint32_t));
         h.off_clock = section(clocks.data(), clocks.size() * sizeof(uint16_t));
         h.off_loc_desc = section(loc_desc.data(), loc_desc.size() * sizeof(uint64_t));
+        h.off_loc_inv1 = section(loc_inv1.data(), loc_inv1.size() * sizeof(uint32_t));
         while (out.size() % 16) out.push_back(0);
         h.total_bytes = static_cast<uint32_t>(out.size());
         std::memcpy(out.data(), &h, sizeof h);
@@ -868,6 +903,18 @@ class Packer {
     }
 
     uint32_t program(std::vector<uint64_t> p, uint32_t tag, uint32_t flags, uint32_t depth) {
+        auto push = [](uint64_t i) {
+            const uint32_t o = CSMC_INS_OP(i);
+            return o == CSMC_OP_PUSH_C || o == CSMC_OP_PUSH_V;
+        };
+        auto binop = [](uint64_t i) {
+            const uint32_t o = CSMC_INS_OP(i);
+            return o == CSMC_OP_ADD || o == CSMC_OP_SUB || o == CSMC_OP_MUL || o == CSMC_OP_DIV ||
+                   o == CSMC_OP_TADD || o == CSMC_OP_TSUB || o == CSMC_OP_TMUL;
+        };
+        if ((p.size() == 3 && push(p[0]) && push(p[1]) && binop(p[2])) ||
+            (p.size() == 5 && push(p[0]) && push(p[1]) && binop(p[2]) && push(p[3]) && binop(p[4])))
+            flags |= CSMC_PROG_CHAIN;
         p.insert(p.begin(), CSMC_INS(CSMC_OP_HDR, flags | (depth << 8)));
         p.push_back(CSMC_INS(CSMC_OP_END, 0));
         std::vector<uint64_t> key = p;

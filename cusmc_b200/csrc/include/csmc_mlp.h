@@ -11,14 +11,19 @@
  * over proposal) in FP64, so weight * goal indicator is an unbiased estimate
  * of the goal probability.
  *
- * Features of a component (CSMC_MLP_IN = 16 inputs, 10 used):
+ * Features of a component (CSMC_MLP_IN = 16 inputs, 10 used), from a
+ * per-network feature source (MlpFeatures):
  *   [0..3]  one-hot of its local location index modulo 4
- *   [4]     its clock value / T (0: components carry no clock feature in
- *           this build; the slot is kept so trained networks stay valid)
- *   [5..8]  integer variables 0..3 divided by the number of components
- *           (for the epidemic network: the S, E, I, R fractions)
- *   [9]     time / T
- * rounded to BF16.  All components in the same local location share their
+ *   [4]     the value of the network's chosen clock variable / T, rounded
+ *           down to a multiple of 1/CSMC_MLP_TIME_STEPS (0 when the network
+ *           chooses none; one clock shared by every component, so the
+ *           components of a location class keep sharing their features)
+ *   [5..8]  four chosen variables times their scales (default: variables
+ *           0..3 times 1/C, for the epidemic network the S, E, I, R
+ *           fractions; 0 for an unused slot)
+ *   [9]     time / T rounded down to a multiple of 1/CSMC_MLP_TIME_STEPS
+ * rounded to BF16 (the time feature takes 64 values over the horizon, so the
+ * network is evaluated again at most 64 times per run because time passed).  All components in the same local location share their
  * features, so a run needs one network evaluation per location class and
  * step.
  *
@@ -39,6 +44,7 @@
 #define CSMC_MLP_FEATURES 10
 #define CSMC_MLP_THETA_MAX 4.0f
 #define CSMC_MLP_CLASSES 4
+#define CSMC_MLP_TIME_STEPS 64.0f
 
 namespace csmc {
 
@@ -116,15 +122,46 @@ CSMC_HD void gelu_both(float x, float &g, float &dg) {
     dg = f_fma(f_mul(x, ds), dz, s);
 }
 
-/* Features of location class l (local index modulo 4) given the run's
- * variables v[0..3] (n_int of them present), components C, time t and
+/* Where a network's features come from: var[i] >= 0 feeds feature 5 + i as
+ * value * scale[i]; clock_var >= 0 feeds feature 4. */
+struct MlpFeatures {
+    int32_t var[4];
+    float scale[4];
+    int32_t clock_var;
+    int32_t pad[3];
+};
+
+/* The default source: variables 0..3 (those that exist) over C components,
+ * no clock. */
+CSMC_HD MlpFeatures mlp_default_features(uint32_t n_vars, uint32_t C) {
+    MlpFeatures F;
+    const float inv_c = f_div(1.0f, static_cast<float>(C));
+    for (int i = 0; i < 4; ++i) {
+        F.var[i] = static_cast<uint32_t>(i) < n_vars ? i : -1;
+        F.scale[i] = inv_c;
+    }
+    F.clock_var = -1;
+    F.pad[0] = F.pad[1] = F.pad[2] = 0;
+    return F;
+}
+
+/* t / T rounded down to a multiple of 1/CSMC_MLP_TIME_STEPS (t >= 0, so
+ * the truncation is the floor; the multiples up to 1 are exact in BF16). */
+CSMC_HD float mlp_time_feature(float t, float T) {
+    const float steps = static_cast<float>(static_cast<int>(f_mul(f_div(t, T), CSMC_MLP_TIME_STEPS)));
+    return bf16_round(f_div(steps, CSMC_MLP_TIME_STEPS));
+}
+
+/* Features of location class l (local index modulo 4): v[i] the value of
+ * F.var[i] (ignored when unused), clk the value of F.clock_var, time t,
  * horizon T; BF16-rounded. */
-CSMC_HD void mlp_features(uint32_t l, const float *v, uint32_t n_int, uint32_t C, float t, float T, float *x) {
+CSMC_HD void mlp_features(uint32_t l, const MlpFeatures &F, const float *v, float clk, float t, float T, float *x) {
     for (int i = 0; i < CSMC_MLP_IN; ++i) x[i] = 0.0f;
     x[l & 3u] = 1.0f;
-    const float inv_c = f_div(1.0f, static_cast<float>(C));
-    for (uint32_t i = 0; i < 4 && i < n_int; ++i) x[5 + i] = bf16_round(f_mul(v[i], inv_c));
-    x[9] = bf16_round(f_div(t, T));
+    if (F.clock_var >= 0) x[4] = mlp_time_feature(clk, T);
+    for (int i = 0; i < 4; ++i)
+        if (F.var[i] >= 0) x[5 + i] = bf16_round(f_mul(v[i], F.scale[i]));
+    x[9] = mlp_time_feature(t, T);
 }
 
 /* Sums in the order of a 32-lane warp.  A run is simulated by one warp:

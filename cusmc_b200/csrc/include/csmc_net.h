@@ -56,6 +56,10 @@ enum csmc_opcode {
  * stack entries (postfix programs without skips, trees of depth <= 2), so it
  * can be evaluated with two registers. */
 #define CSMC_PROG_WINDOW 1u
+/* CHAIN: the program is x1 x2 op or x1 x2 op x3 op (x: PUSH_C / PUSH_V; op:
+ * ADD SUB MUL DIV or TADD TSUB TMUL), a left fold of at most two binary
+ * operations that kernels evaluate without the interpreter. */
+#define CSMC_PROG_CHAIN 2u
 
 #define CSMC_INS(op, a) ((uint64_t)(op) | ((uint64_t)(a) << 8))
 #define CSMC_INS_OP(i) ((uint32_t)((i)&0xffu))
@@ -86,7 +90,7 @@ typedef struct {
     uint32_t off_clock;      /* uint16 id per clock variable (n_clocks entries) */
     uint32_t off_loc_desc;   /* uint64 delay descriptor per location (CSMC_DESC_*) */
     uint32_t n_classes;      /* race classes in use (with CSMC_NET_RACE_CLASSES; 0: not recorded) */
-    uint32_t reserved;
+    uint32_t off_loc_inv1;   /* uint32 per location: its one invariant (CSMC_DESC_INV1), or 0 */
 } csmc_net_header; /* 160 bytes */
 
 /* Header flags. */
@@ -110,6 +114,13 @@ typedef struct {
 #define CSMC_DESC_ZERO (1u << 1)  /* branch / urgent / committed: delay 0 */
 #define CSMC_DESC_INV (1u << 2)   /* has delay-bounding invariants */
 #define CSMC_DESC_EVAL (1u << 3)  /* rate evaluated per component (no table) */
+/* INV1 (with INV): the location's only delay-bounding invariant is clock var
+ * < or <= a literal; loc_inv1[] holds var << 16 | strict << 15 | the
+ * literal's const index (< 2^15).  Never set together with EVAL. */
+#define CSMC_DESC_INV1 (1u << 4)
+#define CSMC_INV1_VAR(w) ((w) >> 16)
+#define CSMC_INV1_STRICT(w) (((w) >> 15) & 1u)
+#define CSMC_INV1_CONST(w) ((w)&0x7fffu)
 /* Race class (high word bits 8..15; 0xff: none): locations whose delay is
  * always exponential with 1/rate from the same literal or the same per-step
  * rate program.  Within a class the delay is a non-increasing function of

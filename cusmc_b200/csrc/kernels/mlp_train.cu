@@ -4,21 +4,27 @@
 // with respect to every parameter, both with BF16 operands and FP32
 // accumulation in tensor memory.
 //
-// One CTA of 128 threads (one warpgroup) walks row tiles of 128 rows; thread
-// t owns row t of the tile, which is also TMEM lane t, so every thread reads
-// its own row's accumulators back with tcgen05.ld.  Per tile:
+// One CTA of 512 threads (four warpgroups) walks row tiles of 128 rows.
+// Thread (g, r), g = warpgroup, r = thread index within it, owns row r of
+// the tile (TMEM lane r; warp w reads TMEM lanes 32 (w mod 4) ..) and columns
+// 16 g .. 16 g + 15 of each 64-wide layer, so the CUDA-core epilogues (GELU,
+// GELU', the BF16 repacking) are spread over 16 warps.  Per tile:
 //   D1 = X  . W1^T          (M=128, N=64,  K=16)   first layer
 //   D2 = H1 . W2^T          (M=128, N=64,  K=64)   second layer
 //   D1 = dZ2 . W2           (M=128, N=64,  K=64)   back-propagation into layer 1
 //   D4 += [dZ2 | dZ1]^T . [H1 | X | 1]   (M=128, N=96, K=128 rows)
 // so D4 accumulates dW2^T, dW1^T and the bias gradients over every tile the
-// CTA processes; the output layer's gradient is accumulated on CUDA cores.
-// Operands live in shared memory in the no-swizzle K-major canonical layout
-// (8-row x 16-byte core matrices; core matrix (row group g, K chunk c) at
-// ((c * rows/8) + g) * 128 bytes), one thread issues the MMAs, completion is
-// signalled through an mbarrier, and every wait is bounded: on a timeout the
-// kernel records an error, waits (bounded) for its MMAs, frees its tensor
-// memory and returns.
+// CTA processes.  A row's theta is the sum of its four groups' partial dot
+// products (exchanged through shared memory, added in group order); the
+// GELU derivatives stay in the registers of the thread that computed them,
+// and the output layer's gradient is accumulated per thread in registers
+// and reduced once at the end in a fixed order (the gradient is
+// deterministic).  Operands live in shared memory in the no-swizzle K-major
+// canonical layout (8-row x 16-byte core matrices; core matrix (row group g,
+// K chunk c) at ((c * rows/8) + g) * 128 bytes), one thread issues the MMAs,
+// completion is signalled through an mbarrier, and every wait is bounded: on
+// a timeout the kernel records an error, waits (bounded) for its MMAs, frees
+// its tensor memory and returns.
 #include "../include/csmc_mlp.h"
 #include "sim.cuh"
 
@@ -28,27 +34,34 @@ namespace csmc {
 namespace {
 
 constexpr int kRows = 128;                      // rows per tile
+constexpr int kGroups = 4;                      // warpgroups per CTA
+constexpr int kThreads = 128 * kGroups;
+constexpr int kCols = CSMC_MLP_HID / kGroups;   // layer columns per thread (16)
 constexpr uint32_t kTmemCols = 256;             // D1/D3 [0,64), D2 [64,128), D4 [128,224)
 constexpr uint32_t kColD1 = 0, kColD2 = 64, kColD4 = 128;
 constexpr int kN4 = 96;                         // [H1 (64) | X (16) | 1 | 0 x 15]
 
-// shared-memory carve-up (bytes); every operand tile ends before kGz1, and
-// the allocation extends 66 KB beyond it, so operand accesses stay inside
-// the allocation even under a transposed reading of the descriptor strides
+// shared-memory carve-up (bytes).  The dZ2 tile (A3) reuses the H1 tile's
+// space (A2): the layer-2 MMA that reads A2 has completed before the
+// epilogue writes A3, and the next tile writes A2 only after the MMA that
+// reads A3 has completed.  The allocation extends far beyond the last
+// operand tile (kSmemBytes), so operand accesses stay inside it even under a
+// transposed reading of the descriptor strides.
 constexpr uint32_t kA1 = 0;                     // X tile      128 x 16
 constexpr uint32_t kB1 = kA1 + 128 * 16 * 2;    // W1          64 x 16
-constexpr uint32_t kA2 = kB1 + 64 * 16 * 2;     // H1 tile     128 x 64
+constexpr uint32_t kA2 = kB1 + 64 * 16 * 2;     // H1 tile     128 x 64; later dZ2 (A3)
+constexpr uint32_t kA3 = kA2;
 constexpr uint32_t kB2 = kA2 + 128 * 64 * 2;    // W2          64 x 64 (out x in)
-constexpr uint32_t kA3 = kB2 + 64 * 64 * 2;     // dZ2 tile    128 x 64
-constexpr uint32_t kB3 = kA3 + 128 * 64 * 2;    // W2^T        64 x 64 (in x out)
+constexpr uint32_t kB3 = kB2 + 64 * 64 * 2;     // W2^T        64 x 64 (in x out)
 constexpr uint32_t kA4 = kB3 + 64 * 64 * 2;     // dZ^T        128 x 128 (neuron x row)
 constexpr uint32_t kB4 = kA4 + 128 * 128 * 2;   // F^T         96 x 128 (feature x row)
-constexpr uint32_t kGz1 = kB4 + kN4 * 128 * 2;  // GELU'(z1) per thread, interleaved: 64 x 128 floats
-constexpr uint32_t kGz2 = kGz1 + 64 * 128 * 4;  // GELU'(z2) per thread, interleaved: 64 x 128 floats
-constexpr uint32_t kMisc = kGz2 + 64 * 128 * 4;  // mbarrier, tmem address, biases, reductions
+constexpr uint32_t kTh = kB4 + kN4 * 128 * 2;   // theta partials [group][row] (floats)
+constexpr uint32_t kMisc = kTh + kGroups * 128 * 4;  // mbarrier, tmem address, biases, reductions
 constexpr uint32_t kMiscBytes = 4096;
-constexpr uint32_t kRedStride = 68;             // per-warp output-layer sums: dw3 (64), db3, pad
-constexpr uint32_t kSmemBytes = kMisc + kMiscBytes;
+constexpr uint32_t kRedStride = 17;             // per-warp output-layer sums: 16 columns, db3
+constexpr uint32_t kSmemBytes = 160 * 1024;     // >= the operands' extent under either stride reading
+static_assert(kMisc + kMiscBytes <= kSmemBytes, "shared-memory carve-up");
+static_assert(1536 + 16 * kRedStride * 4 <= kMiscBytes, "reduction slots");
 
 constexpr uint32_t kWaitLimit = 1u << 20;       // bounded mbarrier polls
 
@@ -136,19 +149,20 @@ __device__ __forceinline__ bool wait_all(uint32_t mbar, uint32_t &phase) {
 // gradient partials per CTA: D4 (128 x 96 floats: row m = output neuron of
 // [layer 2 | layer 1], column n = input [h1 | x | 1 | 0]), dw3 (64), db3, 0.
 template <int MODE>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     mlp_tc_kernel(const MlpRow *rows, uint64_t n_rows, const MlpParams *P, float *theta_out, float *partials,
                   double *objective, int *error) {
     extern __shared__ __align__(1024) uint8_t sm[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t grp = tid >> 7, r = tid & 127u;  // warpgroup, row within the tile
+    const uint32_t c0 = grp * kCols;                // this thread's first layer column
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kMisc);
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(sm + kMisc + 8);
-    float *red = reinterpret_cast<float *>(sm + kMisc + 1536);  // [warp][kRedStride]: dw3 (64), db3
     float *b1s = reinterpret_cast<float *>(sm + kMisc + 512);
     float *b2s = reinterpret_cast<float *>(sm + kMisc + 768);
     float *w3s = reinterpret_cast<float *>(sm + kMisc + 1024);
-    float *gz1 = reinterpret_cast<float *>(sm + kGz1);          // [64][128]
-    float *gz2 = reinterpret_cast<float *>(sm + kGz2);          // [64][128]
+    float *red = reinterpret_cast<float *>(sm + kMisc + 1536);  // [warp][kRedStride]
+    float *thp = reinterpret_cast<float *>(sm + kTh);           // [group][row]
     const uint32_t mbar_a = smem_u32(mbar);
 
     // ---- constant operands: W1 (B1), W2 (B2), W2^T (B3), the ones column of B4
@@ -161,13 +175,12 @@ __global__ void __launch_bounds__(128, 1)
         *reinterpret_cast<uint16_t *>(sm + kB2 + kmaj(o, in, 64)) = P->w2[o][in];
         *reinterpret_cast<uint16_t *>(sm + kB3 + kmaj(in, o, 64)) = P->w2[o][in];
     }
-    for (uint32_t nn = 80; nn < kN4; ++nn) st_bf16(sm + kB4, kmaj(nn, tid, kN4), nn == 80 ? 1.0f : 0.0f);
+    for (uint32_t nn = 80 + grp * 4; nn < 84 + grp * 4; ++nn) st_bf16(sm + kB4, kmaj(nn, r, kN4), nn == 80 ? 1.0f : 0.0f);
     if (tid < 64) {
         b1s[tid] = P->b1[tid];
         b2s[tid] = P->b2[tid];
         w3s[tid] = P->w3[tid];
     }
-    for (uint32_t i = tid; i < 4 * kRedStride; i += blockDim.x) red[i] = 0.0f;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -182,28 +195,34 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tmem_holder;
-    const uint32_t lane_base = (warp * 32u) << 16;  // this warp's TMEM lanes
+    const uint32_t lane_base = ((warp & 3u) * 32u) << 16;  // this warp's TMEM lanes (rows)
     const float b3 = P->b3;
     double J = 0.0;
+    float dw3[kCols];  // this thread's rows' g * h2 for its columns, over all tiles
+#pragma unroll
+    for (int i = 0; i < kCols; ++i) dw3[i] = 0.0f;
+    float db3 = 0.0f;
     uint32_t phase = 0;
     bool ok = true, first = true;
 
     const uint64_t tiles = (n_rows + kRows - 1) / kRows;
     for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint64_t r = tile * kRows + tid;
-        const bool valid = r < n_rows;
+        const uint64_t row_i = tile * kRows + r;
+        const bool valid = row_i < n_rows;
         MlpRow row;
         if (valid) {
-            row = rows[r];
+            row = rows[row_i];
         } else {
 #pragma unroll
             for (int i = 0; i < 16; ++i) row.x[i] = 0;
             row.a = row.b = 0.0f;
         }
+        // each group stores four of the row's sixteen features
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            *reinterpret_cast<uint16_t *>(sm + kA1 + kmaj(tid, i, kRows)) = row.x[i];
-            if (MODE == 1) *reinterpret_cast<uint16_t *>(sm + kB4 + kmaj(64 + i, tid, kN4)) = row.x[i];
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t f = grp * 4u + i;
+            *reinterpret_cast<uint16_t *>(sm + kA1 + kmaj(r, f, kRows)) = row.x[f];
+            if (MODE == 1) *reinterpret_cast<uint16_t *>(sm + kB4 + kmaj(64 + f, r, kN4)) = row.x[f];
         }
         fence_async_smem();
         tc_before_sync();
@@ -216,22 +235,18 @@ __global__ void __launch_bounds__(128, 1)
             mma_commit(mbar_a);
         }
         if (!(ok = wait_all(mbar_a, phase))) break;
+        float dg1[kCols];  // GELU'(z1) of this thread's columns
         {
             float z[16];
+            tmem_ld16(tmem + lane_base + kColD1 + c0, z);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                tmem_ld16(tmem + lane_base + kColD1 + 16 * c, z);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int j = 16 * c + i;
-                    const float zz = f_add(z[i], b1s[j]);
-                    float gv, dg;
-                    gelu_both(zz, gv, dg);
-                    const float h = bf16_round(gv);
-                    if (MODE == 1) gz1[j * 128 + tid] = dg;
-                    st_bf16(sm + kA2, kmaj(tid, j, kRows), h);
-                    if (MODE == 1) st_bf16(sm + kB4, kmaj(j, tid, kN4), h);
-                }
+            for (int i = 0; i < kCols; ++i) {
+                const uint32_t j = c0 + i;
+                float gv;
+                gelu_both(f_add(z[i], b1s[j]), gv, dg1[i]);
+                const float h = bf16_round(gv);
+                st_bf16(sm + kA2, kmaj(r, j, kRows), h);
+                if (MODE == 1) st_bf16(sm + kB4, kmaj(j, r, kN4), h);
             }
         }
         fence_async_smem();
@@ -247,46 +262,39 @@ __global__ void __launch_bounds__(128, 1)
             mma_commit(mbar_a);
         }
         if (!(ok = wait_all(mbar_a, phase))) break;
-        float z2[64];
+        float h2[kCols], dg2[kCols];
+        {
+            float z2[16];
+            tmem_ld16(tmem + lane_base + kColD2 + c0, z2);
+            float part = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) tmem_ld16(tmem + lane_base + kColD2 + 16 * c, z2 + 16 * c);
-        float th = b3;
-#pragma unroll
-        for (int k = 0; k < 64; ++k) {  // z2[k] becomes GELU(z2 + b2); the derivative goes to gz2
-            float gv, dg;
-            gelu_both(f_add(z2[k], b2s[k]), gv, dg);
-            z2[k] = gv;
-            if (MODE == 1) gz2[k * 128 + tid] = dg;
-            th = f_fma(gv, w3s[k], th);
+            for (int i = 0; i < kCols; ++i) {
+                gelu_both(f_add(z2[i], b2s[c0 + i]), h2[i], dg2[i]);
+                part = f_fma(h2[i], w3s[c0 + i], part);
+            }
+            thp[grp * 128 + r] = part;
         }
+        __syncthreads();
+        const float th = f_add(f_add(f_add(f_add(b3, thp[r]), thp[128 + r]), thp[256 + r]), thp[384 + r]);
         const bool inside = th >= -CSMC_MLP_THETA_MAX && th <= CSMC_MLP_THETA_MAX;
         const float thc = inside ? th : (th < 0.0f ? -CSMC_MLP_THETA_MAX : CSMC_MLP_THETA_MAX);
         if (MODE == 0) {
-            if (valid) theta_out[r] = thc;
+            if (valid && grp == 0) theta_out[row_i] = thc;
             tc_before_sync();
             __syncthreads();
             continue;
         }
         const float e = exp2_f(f_mul(thc, 1.44269502f));
-        if (valid) J += static_cast<double>(row.b) * thc - static_cast<double>(row.a) * e;
+        if (valid && grp == 0) J += static_cast<double>(row.b) * thc - static_cast<double>(row.a) * e;
         const float g = (valid && inside) ? f_add(row.b, -f_mul(row.a, e)) : 0.0f;
-        // output layer: dw3 += g h2, db3 += g (warp sums into the warp's own
-        // slots; the four warps' slots are added in a fixed order at the end,
-        // so the gradient does not depend on warp timing)
-        float *rw = red + warp * kRedStride;
-        float gs = g;
+        if (grp == 0) db3 = f_add(db3, g);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, o);
-        if (lane == 0) rw[64] += gs;
-#pragma unroll
-        for (int k = 0; k < 64; ++k) {
-            float v = f_mul(g, z2[k]);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) rw[k] += v;
-            const float dz = f_mul(f_mul(g, w3s[k]), gz2[k * 128 + tid]);
-            st_bf16(sm + kA3, kmaj(tid, k, kRows), dz);
-            st_bf16(sm + kA4, kmaj(k, tid, kRows), dz);
+        for (int i = 0; i < kCols; ++i) {
+            const uint32_t k = c0 + i;
+            dw3[i] = f_fma(g, h2[i], dw3[i]);
+            const float dz = f_mul(f_mul(g, w3s[k]), dg2[i]);
+            st_bf16(sm + kA3, kmaj(r, k, kRows), dz);
+            st_bf16(sm + kA4, kmaj(k, r, kRows), dz);
         }
         fence_async_smem();
         tc_before_sync();
@@ -303,15 +311,9 @@ __global__ void __launch_bounds__(128, 1)
         if (!(ok = wait_all(mbar_a, phase))) break;
         {
             float dh[16];
+            tmem_ld16(tmem + lane_base + kColD1 + c0, dh);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                tmem_ld16(tmem + lane_base + kColD1 + 16 * c, dh);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int j = 16 * c + i;
-                    st_bf16(sm + kA4, kmaj(64 + j, tid, kRows), f_mul(dh[i], gz1[j * 128 + tid]));
-                }
-            }
+            for (int i = 0; i < kCols; ++i) st_bf16(sm + kA4, kmaj(64 + c0 + i, r, kRows), f_mul(dh[i], dg1[i]));
         }
         fence_async_smem();
         tc_before_sync();
@@ -336,24 +338,46 @@ __global__ void __launch_bounds__(128, 1)
 
     if (MODE == 1) {
         float *out = partials + static_cast<size_t>(blockIdx.x) * (128 * kN4 + 66);
-        if (ok && !first) {  // block-uniform
-            float v[16];
+        if (grp < 3) {  // groups 0..2 read 32 of D4's 96 columns each
+            if (ok && !first) {  // block-uniform
+                float v[16];
 #pragma unroll
-            for (int c = 0; c < kN4 / 16; ++c) {
-                tmem_ld16(tmem + lane_base + kColD4 + 16 * c, v);
+                for (int c = 0; c < 2; ++c) {
+                    const uint32_t col = grp * 32u + 16u * c;
+                    tmem_ld16(tmem + lane_base + kColD4 + col, v);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) out[tid * kN4 + 16 * c + i] = v[i];
+                    for (int i = 0; i < 16; ++i) out[r * kN4 + col + i] = v[i];
+                }
+            } else {
+                for (int i = 0; i < 32; ++i) out[r * kN4 + grp * 32 + i] = 0.0f;
             }
-        } else {
-            for (int i = 0; i < kN4; ++i) out[tid * kN4 + i] = 0.0f;
         }
+        // output layer: per warp, the sum over its 32 rows (butterfly), then
+        // the four warps of a group in warp order
+#pragma unroll
+        for (int i = 0; i < kCols; ++i) {
+            float v = dw3[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp * kRedStride + i] = v;
+        }
+        float vb = db3;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vb += __shfl_xor_sync(0xffffffffu, vb, o);
+        if (lane == 0) red[warp * kRedStride + kCols] = vb;
         __syncthreads();
-        if (tid < 65)
+        if (tid < 64) {  // dw3[k]: group k / 16, its warps 4g .. 4g + 3
+            const uint32_t gk = tid / kCols, i = tid % kCols;
+            const float *rw = red + (4 * gk) * kRedStride + i;
             out[128 * kN4 + tid] =
-                f_add(f_add(f_add(red[tid], red[kRedStride + tid]), red[2 * kRedStride + tid]), red[3 * kRedStride + tid]);
+                f_add(f_add(f_add(rw[0], rw[kRedStride]), rw[2 * kRedStride]), rw[3 * kRedStride]);
+        }
+        if (tid == 64)
+            out[128 * kN4 + 64] = f_add(f_add(f_add(red[kCols], red[kRedStride + kCols]), red[2 * kRedStride + kCols]),
+                                        red[3 * kRedStride + kCols]);
         if (tid == 65) out[128 * kN4 + 65] = 0.0f;
         __shared__ double jred[128];
-        jred[tid] = J;
+        if (grp == 0) jred[r] = J;
         __syncthreads();
         if (tid == 0) {
             double sum = 0.0;
@@ -379,12 +403,12 @@ int mlp_tc_launch(int mode, const MlpRow *rows, uint64_t n_rows, const MlpParams
         auto fn = mlp_tc_kernel<0>;
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         if (e != cudaSuccess) return static_cast<int>(e);
-        fn<<<grid, 128, kSmemBytes, st>>>(rows, n_rows, P, theta_out, partials, objective, error);
+        fn<<<grid, kThreads, kSmemBytes, st>>>(rows, n_rows, P, theta_out, partials, objective, error);
     } else {
         auto fn = mlp_tc_kernel<1>;
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         if (e != cudaSuccess) return static_cast<int>(e);
-        fn<<<grid, 128, kSmemBytes, st>>>(rows, n_rows, P, theta_out, partials, objective, error);
+        fn<<<grid, kThreads, kSmemBytes, st>>>(rows, n_rows, P, theta_out, partials, objective, error);
     }
     return static_cast<int>(cudaGetLastError());
 }

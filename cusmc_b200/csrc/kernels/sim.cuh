@@ -26,6 +26,11 @@
 #include "../include/csmc_numeric.h"
 #include "../include/csmc_mlp.h"
 
+// Tilt groups of the thread-per-run importance-sampling kernel: 3-bit
+// location codes 0..5 (6 pads the last location word, 7 is the descriptor
+// path).
+#define CSMC_IS_GROUPS 6
+
 namespace csmc {
 
 // Section offsets and counts of the packed network (copied from its header
@@ -35,7 +40,7 @@ struct NetLayout {
     uint32_t off_loc_rate, off_inv_lit, off_rate_prog, off_clock, off_loc_desc;
     uint32_t n_comps, n_vars, n_rate_prog, flags, n_clocks, recv_lo, recv_hi;
     uint32_t n_classes;  // race classes in use (CSMC_RACE_CLASSES when the blob does not record it)
-    uint32_t pad;
+    uint32_t off_loc_inv1;  // one-invariant table (0: none)
 };
 
 inline NetLayout layout_of(const csmc_net_header &h) {
@@ -44,7 +49,7 @@ inline NetLayout layout_of(const csmc_net_header &h) {
                      h.off_var,      h.off_const,   h.off_code,      h.off_loc_rate, h.off_inv_lit,
                      h.off_rate_prog, h.off_clock,  h.off_loc_desc,  h.n_comps,      h.n_vars,
                      h.n_rate_prog,  h.flags,       h.n_clocks,      h.recv_chan_lo, h.recv_chan_hi,
-                     ncls,           0u};
+                     ncls,           h.off_loc_inv1};
 }
 
 struct SimParams {
@@ -73,7 +78,10 @@ struct SimParams {
                                   // (null: state in shared memory after the network)
     PhiloxKeys keys;              // round keys of the seed (philox_keys(seed)): read from the
                                   // parameter bank by the class-coded kernel
+    uint32_t class_src[CSMC_RACE_CLASSES];  // class-coded kernel: each race class's 1/rate,
+                                  // CSMC_CLASS_SRC_PROG | rate-table slot, or the literal's float bits
 };
+#define CSMC_CLASS_SRC_PROG 0x80000000u
 
 #define CSMC_SCRATCH_WORDS 8
 
@@ -95,12 +103,17 @@ int serial_max_active_ctas(bool verify, bool slots, bool loc8, bool gstate, bool
 // Class-coded thread-per-run kernel (sim_coded.cuh): networks with race
 // classes, at most 256 components and at most 32 locations per automaton,
 // run state in shared memory.
-int coded_launch(bool verify, bool slots, const SimParams &p, int grid, int block, size_t smem, void *stream);
-int coded_max_active_ctas(bool verify, bool slots, int block, size_t smem, int *ctas);
-// Bytes of a T-thread state slab of the class-coded kernel (carve_coded_view).
-inline size_t coded_slab_bytes(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots, uint32_t T) {
-    size_t b = (4u * (2u * n_vars + n_rate_prog) * static_cast<size_t>(T) + 7u) & ~static_cast<size_t>(7);
-    b += 8u * 4u * CSMC_RACE_CLASSES * static_cast<size_t>(T);     // class keys: (largest, second) per chain
+// all_classed: every location of the network belongs to a race class.
+int coded_launch(bool verify, bool slots, bool all_classed, const SimParams &p, int grid, int block, size_t smem,
+                 void *stream);
+int coded_max_active_ctas(bool verify, bool slots, bool all_classed, int block, size_t smem, int *ctas);
+// Bytes of a T-thread state slab of the class-coded kernel
+// (carve_coded_view): n_classes race classes, recv: the network has
+// receiving edges (the receiver snapshot is kept).
+inline size_t coded_slab_bytes(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots, uint32_t T,
+                               uint32_t n_classes, bool recv) {
+    size_t b = 4u * ((recv ? 2u : 1u) * n_vars + n_rate_prog) * static_cast<size_t>(T);
+    b += 4u * 4u * n_classes * static_cast<size_t>(T);             // class keys: the largest of each chain
     b += 4u * ((n_comps + 3u) / 4u) * static_cast<size_t>(T);        // location words
     if (slots) b += 4u * n_comps * static_cast<size_t>(T);          // enabled-edge slot masks
     return (b + 15u) & ~static_cast<size_t>(15);
@@ -135,21 +148,50 @@ struct BatchJob {
 };
 static_assert(sizeof(BatchJob) % 16 == 0, "BatchJob is copied in 16-byte words");
 
+// Job table: the n_group_jobs warp-per-run jobs first, then the thread-per-
+// run jobs; each part sorted by run_begin within its own run space.
 struct BatchParams {
-    const BatchJob *jobs;          // device job table, sorted by run_begin
+    const BatchJob *jobs;          // device job table
     uint32_t n_jobs;
-    uint32_t state_stride;         // bytes of one CTA's state slab
-    uint64_t total_runs;
-    unsigned long long *queue;     // the shared run counter
+    uint32_t state_stride;         // bytes of one CTA's thread-per-run state slab
+    uint64_t total_runs;           // runs of the thread-per-run jobs
+    unsigned long long *queue;     // the thread-per-run jobs' run counter
     uint8_t *state;                // grid * state_stride bytes
-    uint32_t max_vars, max_rate_prog, max_comps, pad;
+    uint32_t max_vars, max_rate_prog, max_comps;  // maxima over the thread-per-run jobs
+    uint32_t n_group_jobs;         // jobs simulated one warp per run (0: none)
+    uint64_t group_runs;           // runs of the warp-per-run jobs
+    unsigned long long *group_queue;  // their run counter (null when n_group_jobs is 0)
+    uint32_t group_stride;         // shared memory of one warp's run state (group_state_stride over the jobs)
+    uint32_t group_k;              // components per lane of the warp-per-run jobs: 4, 8 or 16
 };
 
 #define CSMC_BATCH_MAX_JOBS 256
+// Largest network a batch job can run one warp per run: 32 lanes x 16
+// components.
+#define CSMC_BATCH_GROUP_MAX_COMPS 512
 
 int batch_launch(bool verify, const BatchParams &p, int grid, int block, void *stream);
-int batch_max_active_ctas(bool verify, int block, size_t smem, int *ctas);
+// group_k: 0 (thread per run only) or the components per lane of the
+// warp-per-run jobs (4, 8 or 16)
+int batch_max_active_ctas(bool verify, int group_k, int block, size_t smem, int *ctas);
 inline size_t batch_smem_bytes(uint32_t n_jobs) { return static_cast<size_t>(n_jobs) * sizeof(BatchJob); }
+// Shared memory of a batch launch: the job table, then one warp-per-run
+// state per warp when some job runs one warp per run.
+inline size_t batch_smem_bytes(uint32_t n_jobs, uint32_t group_stride, int block) {
+    return batch_smem_bytes(n_jobs) + (group_stride ? static_cast<size_t>(block / 32) * group_stride : 0);
+}
+// Shared memory of one lane group's run state (sim_impl.cuh: RunState): 48
+// bytes of scalars, the variables and one inverse rate per rate program,
+// 16-aligned; then the group's slot masks, component gl*K + k of lane gl at
+// [k * lanes + gl].
+__host__ __device__ inline uint32_t group_vars_bytes(uint32_t n_vars, uint32_t n_rate_prog) {
+    return (48u + 4u * (n_vars + n_rate_prog) + 15u) & ~15u;
+}
+__host__ __device__ inline uint32_t group_state_stride(uint32_t n_vars, uint32_t n_rate_prog, uint32_t lanes,
+                                                       uint32_t comps_per_lane) {
+    // 16-aligned: the next group's scalars hold doubles
+    return (group_vars_bytes(n_vars, n_rate_prog) + 4u * lanes * comps_per_lane + 15u) & ~15u;
+}
 // Bytes of one thread's state in a batch slab (16-bit locations, slot masks).
 inline size_t batch_state_bytes_per_thread(uint32_t max_comps, uint32_t max_vars, uint32_t max_rate_prog) {
     return 4u * (2u * max_vars + max_rate_prog + 2u * CSMC_RACE_CLASSES) + 2u * max_comps + 4u * max_comps + 4u;
@@ -169,8 +211,35 @@ struct IsParams {
     MlpRow *rows;                 // trace mode: the rows
     uint64_t rows_cap;            // trace mode: rows the buffer holds (writes beyond it are skipped, counted)
     uint32_t slab_bytes;          // shared memory of one warp (is_warp_slab_bytes)
-    uint32_t pad;
+    uint32_t n_groups;            // thread-per-run kernel: tilt groups in use (<= CSMC_IS_GROUPS)
+    MlpFeatures feat;             // where the proposal's features come from
+    // thread-per-run kernel (sim_is_coded.cuh): the tilt groups, i.e. the
+    // (race class, location class) pairs of the network's classed
+    // locations.  group_map holds, at bits 3 (4 g + l), the 3-bit location
+    // code of race class g in location class l: a group index, or 7 (the
+    // descriptor path) for pairs beyond the first CSMC_IS_GROUPS.
+    uint64_t group_map;
+    uint32_t group_l;                       // location class of group i at bits 2i .. 2i + 1
+    uint32_t group_src[CSMC_IS_GROUPS];     // 1/rate source of group i (SimParams::class_src format)
 };
+
+// Importance sampling one thread per run (sim_is_coded.cuh), for networks
+// with race classes (at most 256 components, 32 locations per automaton):
+// the CUDA-core evaluation of theta, no trace mode.  Shared memory: the
+// network, the proposal network's FP32 copies, each warp's first-hidden-layer staging,
+// then is_coded_slab_bytes of run state.
+int is_coded_launch(bool slots, const IsParams &p, int grid, int block, size_t smem, void *stream);
+int is_coded_max_active_ctas(bool slots, int block, size_t smem, int *ctas);
+// Shared memory of the proposal network in that kernel (the FP32 copies).
+size_t is_coded_mlp_smem_bytes();
+// Run state of a CTA of T threads: per thread and tilt group the step's
+// 1/rate, 1/rate' and FP64 rate change (4 words), then the class-coded
+// layout with one key chain set per tilt group.
+inline size_t is_coded_slab_bytes(uint32_t n_comps, uint32_t n_vars, uint32_t n_rate_prog, bool slots, uint32_t T,
+                                  uint32_t n_groups, bool recv) {
+    return 16u * n_groups * static_cast<size_t>(T) + coded_slab_bytes(n_comps, n_vars, n_rate_prog, slots, T,
+                                                                     n_groups, recv);
+}
 
 // tc: theta by warp-level tensor-core MMAs (else the CUDA-core evaluation
 // that is bit-identical to the CPU oracle).
@@ -182,7 +251,9 @@ int is_max_active_ctas(bool tc, bool trace, bool slots, bool loc8, int block, si
 // state (the thread-per-run layout with one thread) and, for the CUDA-core
 // evaluation, the first hidden layer of the step's four rows.
 size_t is_mlp_smem_bytes();
+#ifndef CSMC_IS_BLOCK
 #define CSMC_IS_BLOCK 256  // threads per CTA of the importance-sampling kernel (eight runs)
+#endif
 inline size_t is_warp_slab_bytes(size_t run_state_bytes, bool tc) {
     return (tc ? 0u : 4u * CSMC_MLP_HID * CSMC_MLP_CLASSES) + ((run_state_bytes + 15u) & ~static_cast<size_t>(15));
 }

@@ -1,6 +1,10 @@
 // Multi-network batch kernel: one persistent launch over many (network,
-// query) jobs, each run simulated by one thread with the step of
-// sim_run.cuh.
+// query) jobs.  Runs of small networks are simulated by one thread each
+// with the step of sim_run.cuh; runs of large networks (the jobs the host
+// marks, at most CSMC_BATCH_GROUP_MAX_COMPS components) by one warp each,
+// 32 lanes x K components, with the lane-group run of sim_impl.cuh, so that
+// the long runs of a large network do not leave one thread working alone
+// at the end of the batch.
 //
 // Work queue.  The runs of all jobs are numbered in one index space (job j
 // owns [run_begin_j, run_begin_j + n_runs_j)); a lane whose run ends takes
@@ -10,11 +14,19 @@
 // lane idle until the whole batch is drained.  Lanes of one warp are on the
 // same job except at the few indices where one job ends and the next begins.
 //
+// Warp-per-run jobs have their own run space and counter.  Every warp first
+// takes runs of those (the long ones) until their counter is drained, then
+// joins the thread-per-run queue, so the short runs fill in behind the long
+// ones.
+//
 // Memory.  Networks stay in global memory (read-only, L1/L2-resident while
-// in use); each CTA's run state is a global slab laid out for the largest
-// job of the batch (interleaved by thread, so warp accesses coalesce).
-// Results depend only on the job and the run index.
+// in use); each CTA's thread-per-run state is a global slab laid out for the
+// largest thread-per-run job (interleaved by thread, so warp accesses
+// coalesce); a warp-per-run run keeps its scalars, variables and rate table
+// in shared memory after the job table.  Results depend only on the job and
+// the run index, never on which mode ran it.
 #pragma once
+#include "sim_impl.cuh"
 #include "sim_run.cuh"
 
 namespace csmc {
@@ -22,6 +34,9 @@ namespace detail {
 
 #ifndef CSMC_BATCH_MIN_CTAS_PER_SM
 #define CSMC_BATCH_MIN_CTAS_PER_SM 4
+#endif
+#ifndef CSMC_BATCH_GROUP_MIN_CTAS_PER_SM
+#define CSMC_BATCH_GROUP_MIN_CTAS_PER_SM 3
 #endif
 
 // Index of the job owning run index r: the last job with run_begin <= r.
@@ -43,8 +58,36 @@ static __device__ __forceinline__ void flush_counters(const BatchJob &J, unsigne
     hits = steps = capped = 0;
 }
 
-template <bool VERIFY>
-__global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(const BatchParams p) {
+// Warp-per-run jobs (K components per lane): whole warps take runs from
+// p.group_queue until it passes p.group_runs.  Not inlined, so that its
+// registers are allocated apart from the thread-per-run phase's.
+template <int K, bool VERIFY>
+static __device__ __forceinline__ void batch_group_phase(const BatchParams &p, const BatchJob *jobs, uint8_t *smem) {
+    const uint32_t lane = threadIdx.x & 31u;
+    RunState *s = reinterpret_cast<RunState *>(smem + p.n_jobs * sizeof(BatchJob) + (threadIdx.x >> 5) * p.group_stride);
+    unsigned long long acc_hits = 0, acc_steps = 0, acc_capped = 0;
+    uint32_t jb = 0;
+    for (;;) {
+        unsigned long long r = 0;
+        if (lane == 0) r = atomicAdd(p.group_queue, 1ull);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r >= p.group_runs) break;
+        const uint32_t j = find_job(jobs, p.n_group_jobs, r);
+        if (j != jb) {
+            if (lane == 0) flush_counters(jobs[jb], acc_hits, acc_steps, acc_capped);
+            jb = j;
+        }
+        const BatchJob &J = jobs[jb];
+        const Net n = net_view(J.blob, J.net);
+        const unsigned long long local = r - J.run_begin;
+        group_run<32, K, VERIFY>(n, s, J, J.first_run + local, local, lane, 0u, 0xffffffffu, acc_hits, acc_steps,
+                                 acc_capped);
+    }
+    if (lane == 0) flush_counters(jobs[jb], acc_hits, acc_steps, acc_capped);
+}
+
+template <bool VERIFY, int K>
+__global__ void __launch_bounds__(128, K > 0 ? CSMC_BATCH_GROUP_MIN_CTAS_PER_SM : CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(const __grid_constant__ BatchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     {  // stage the job table
         const uint4 *src = reinterpret_cast<const uint4 *>(p.jobs);
@@ -53,7 +96,12 @@ __global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    const BatchJob *jobs = reinterpret_cast<const BatchJob *>(smem);
+    if constexpr (K > 0) {
+        if (p.n_group_jobs > 0) batch_group_phase<K, VERIFY>(p, reinterpret_cast<const BatchJob *>(smem), smem);
+    }
+    if (p.n_jobs == p.n_group_jobs) return;
+    const BatchJob *jobs = reinterpret_cast<const BatchJob *>(smem) + p.n_group_jobs;
+    const uint32_t n_jobs = p.n_jobs - p.n_group_jobs;
 
     const uint32_t T = blockDim.x, t = threadIdx.x;
     uint8_t *st = p.state + static_cast<size_t>(blockIdx.x) * p.state_stride;
@@ -82,7 +130,7 @@ __global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(
             if (need) {
                 const unsigned long long r = base + __popc(want & ((1u << lane) - 1u));
                 if (r >= p.total_runs) break;
-                const uint32_t j = find_job(jobs, p.n_jobs, r);
+                const uint32_t j = find_job(jobs, n_jobs, r);
                 if (j != jb) {
                     flush_counters(jobs[jb], acc_hits, acc_steps, acc_capped);
                     jb = j;
@@ -129,19 +177,19 @@ __global__ void __launch_bounds__(128, CSMC_BATCH_MIN_CTAS_PER_SM) batch_kernel(
 
 }  // namespace detail
 
-template <bool VERIFY>
+template <bool VERIFY, int K>
 int batch_launch_one(const BatchParams &p, int grid, int block, void *stream) {
-    auto fn = detail::batch_kernel<VERIFY>;
-    const size_t smem = batch_smem_bytes(p.n_jobs);
+    auto fn = detail::batch_kernel<VERIFY, K>;
+    const size_t smem = batch_smem_bytes(p.n_jobs, p.n_group_jobs ? p.group_stride : 0u, block);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     fn<<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return static_cast<int>(cudaGetLastError());
 }
 
-template <bool VERIFY>
+template <bool VERIFY, int K>
 int batch_occupancy_one(int block, size_t smem, int *ctas) {
-    auto fn = detail::batch_kernel<VERIFY>;
+    auto fn = detail::batch_kernel<VERIFY, K>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     return static_cast<int>(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, smem));

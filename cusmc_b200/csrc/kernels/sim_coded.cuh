@@ -8,12 +8,18 @@
 // bytes of components 4q..4q+3 form word q of the thread's state, so one
 // shared load gives the codes of the four components that share Philox
 // block q.  A class member contributes only its key, (24-bit draw) * 256 +
-// (255 - bit-reversed index), to the class's two largest keys; each class
-// keeps four independent pairs, one per word of the Philox block (chain k),
-// so consecutive members of a class do not wait on each other's shared-
-// memory update.  After the components, the pairs of a class are merged and
-// the class takes part in the race with its largest key, exactly as in
-// race_classes (sim_run.cuh); the same cases fall back to race_exact.
+// (255 - bit-reversed index), to its class's largest key; each class keeps
+// four independent maxima, one per word of the Philox block (chain k), so
+// consecutive members of a class do not wait on each other's shared-memory
+// update.  After the components, the chains of a class are merged and the
+// class takes part in the race with its largest key, as in race_classes
+// (sim_run.cuh).  Where race_classes consults the second largest key (a
+// lower draw that rounds to the same float delay could hide a member with a
+// smaller index), this kernel falls back to race_exact whenever the largest
+// draw of a class whose delay is the race's minimum sits on such a flat
+// spot of the delay function (about 2e-4 .. 4e-3 per step for a class of
+// 1-10 members, far less with many); delays do not increase with the
+// draw, so no flat spot means no tie with a lower draw.
 //
 // The Philox blocks of a step are computed through philox_step /
 // philox_block (csmc_numeric.h): the counter words the blocks share are
@@ -33,15 +39,19 @@ namespace detail {
 
 constexpr uint32_t kCodeGeneral = 7u;  // delay through the location's descriptor
 constexpr uint32_t kCodePad = 6u;      // no component
-constexpr uint32_t kKeyWords = 2u * 4u * CSMC_RACE_CLASSES;  // (largest, second) per chain per class
+#ifndef CSMC_CODED_UNROLL
+#define CSMC_CODED_UNROLL 1
+#endif
+constexpr int kCodedUnroll = CSMC_CODED_UNROLL;  // Philox blocks of the race loop in flight per iteration
 
 // Run state of one thread in the class-coded layout: vars[V] | rates[P] |
-// shadow[V] (floats) | class keys (uint2 pairs [class*4 + chain]) |
-// location words [ceil(C/4)] | slots[C] (u32); element i of thread t at
-// [i * T + t] (the key pairs as 8-byte elements).
+// shadow[V] (floats; only for networks with receiving edges, else the
+// snapshot view aliases the variables and is never used) | class keys
+// ([class*4 + chain], NG classes) | location words [ceil(C/4)] | slots[C]
+// (all 4-byte words); element i of thread t at [i * T + t].
 struct CodedView {
     VarView vars, rates, shadow;
-    uint2 *keys;      // this thread's pair 0; stride T
+    uint32_t *keys;   // this thread's chain 0 of class 0; stride T
     uint32_t *lw;     // this thread's location word 0; stride T
     uint32_t *slotv;  // this thread's element 0; stride T
     uint32_t T;
@@ -63,15 +73,15 @@ struct CodedView {
 static __host__ __device__ __forceinline__ uint32_t coded_words(uint32_t C) { return (C + 3u) >> 2; }
 
 static __device__ __forceinline__ CodedView carve_coded_view(uint8_t *st, uint32_t V, uint32_t P, uint32_t C,
-                                                             uint32_t T, uint32_t t) {
+                                                             uint32_t NG, bool recv, uint32_t T, uint32_t t) {
     float *fb = reinterpret_cast<float *>(st);
     CodedView r;
     r.vars = VarView{fb + t, T};
     r.rates = VarView{fb + V * T + t, T};
-    r.shadow = VarView{fb + (V + P) * T + t, T};
-    const uint32_t kb = (4u * (2u * V + P) * T + 7u) & ~7u;
-    r.keys = reinterpret_cast<uint2 *>(st + kb) + t;
-    const uint32_t lb = kb + 4u * kKeyWords * T;
+    r.shadow = recv ? VarView{fb + (V + P) * T + t, T} : r.vars;
+    const uint32_t kb = 4u * ((recv ? 2u : 1u) * V + P) * T;
+    r.keys = reinterpret_cast<uint32_t *>(st + kb) + t;
+    const uint32_t lb = kb + 4u * 4u * NG * T;
     r.lw = reinterpret_cast<uint32_t *>(st + lb) + t;
     r.slotv = reinterpret_cast<uint32_t *>(st + lb + 4u * coded_words(C) * T) + t;
     r.T = T;
@@ -84,86 +94,113 @@ static __device__ __forceinline__ float desc_delay(const Net &n, const CodedView
     const uint64_t dsc = n.loc_desc[li];
     const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
     if (fl & CSMC_DESC_ZERO) return 0.0f;
-    if (fl & (CSMC_DESC_INV | CSMC_DESC_EVAL)) return slow_delay(n, rv.vars, rv.rates, li, x);
+    if (fl & (CSMC_DESC_INV | CSMC_DESC_EVAL)) return bounded_delay(n, rv.vars, rv.rates, li, lo, fl, x);
     const float inv = (fl & CSMC_DESC_PROG) ? rv.rates[lo] : __uint_as_float(lo);
     return exp_delay(x, inv);
 }
 
-// The largest and second largest of four pairs (a_k largest, b_k second
-// largest of chain k; keys of different chains are distinct).
-static __device__ __forceinline__ void merge_chains(const uint2 &p0, const uint2 &p1, const uint2 &p2, const uint2 &p3,
-                                                    uint32_t &m1, uint32_t &m2) {
-    const uint32_t hi01 = max(p0.x, p1.x), lo01 = min(p0.x, p1.x);
-    const uint32_t hi23 = max(p2.x, p3.x), lo23 = min(p2.x, p3.x);
-    m1 = max(hi01, hi23);
-    const uint32_t second_of_firsts = max(max(lo01, lo23), min(hi01, hi23));
-    m2 = max(second_of_firsts, max(max(p0.y, p1.y), max(p2.y, p3.y)));
+// One component's part in the race: a class member updates its class's
+// chain-k pair, any other component (ALLCLS false) races with its own delay.
+// br: the component's bit-reversed index (bitrev_bits(cc, bits)).
+template <bool ALLCLS, uint32_t k>
+static __device__ __forceinline__ void race_member(const Net &n, uint32_t bits, const CodedView &rv, uint32_t wd,
+                                                   uint32_t cc, uint32_t x, uint32_t br, unsigned long long &best,
+                                                   float &bestd) {
+    const uint32_t b = (wd >> (8u * k)) & 0xffu;
+    const uint32_t code = b >> 5;
+    const uint32_t T = rv.T;
+    if (ALLCLS || code < CSMC_RACE_CLASSES) {
+        const uint32_t key = (x | 0xffu) - br;
+        uint32_t *pp = rv.keys + (code * 4u + k) * T;
+        *pp = max(*pp, key);
+    } else if (code == kCodeGeneral) {
+        const float d = desc_delay(n, rv, n.comp[cc].loc_begin + (b & 31u), x);
+        const unsigned long long key = (static_cast<unsigned long long>(delay_key(d)) << 32) | br;
+        if (key < best) {
+            best = key;
+            bestd = d;
+        }
+    }
 }
 
 // The race decided from the class keys (race_classes' decision over the
-// same keys); false: the caller runs race_exact.
+// same keys); false: the caller runs race_exact.  src: each class's 1/rate
+// source (CSMC_CLASS_SRC_PROG | slot, or float bits).  ALLCLS: every
+// location is classed, so no component takes the descriptor path.
+template <bool ALLCLS>
 static __device__ __forceinline__ bool race_coded(const Net &n, uint32_t C, uint32_t bits, uint32_t NG,
-                                                  const CodedView &rv, const PhiloxKeys &K, uint64_t run,
-                                                  uint32_t step, unsigned long long &best, float &bestd) {
+                                                  const CodedView &rv, const PhiloxKeys &K, const uint32_t *src,
+                                                  uint64_t run, uint32_t step, unsigned long long &best,
+                                                  float &bestd) {
     const uint32_t T = rv.T;
-    for (uint32_t w = 0; w < 4u * NG; ++w) rv.keys[w * T] = make_uint2(0u, 0u);
+    for (uint32_t w = 0; w < 4u * NG; ++w) rv.keys[w * T] = 0u;
     best = ~0ull;
     bestd = 0.0f;
     const PhiloxStep ps = philox_step(K, step, run);
-    const uint32_t Q = coded_words(C);
-    for (uint32_t q = 0; q < Q; ++q) {
+    // bit reversal of component 4q + k over `bits` (>= 2) bits: the two low
+    // bits (k) become the top two, q the low bits - 2 reversed
+    const uint32_t hi_shift = bits - 2u;  // bits >= 2: the plan needs at least four components
+    const uint32_t Qf = C >> 2;           // words whose four components all exist
+#pragma unroll kCodedUnroll
+    for (uint32_t q = 0; q < Qf; ++q) {
         const u32x4 blk = philox_block(K, ps, q);
-        const uint32_t wd = rv.lw[q * T];
-#pragma unroll
-        for (uint32_t k = 0; k < 4; ++k) {
-            const uint32_t b = (wd >> (8u * k)) & 0xffu;
-            const uint32_t code = b >> 5;
-            const uint32_t cc = 4u * q + k;
-            const uint32_t x = word_of(blk, k);
-            if (code < CSMC_RACE_CLASSES) {
-                const uint32_t key = (x | 0xffu) - bitrev_bits(cc, bits);
-                uint2 *pp = rv.keys + (code * 4u + k) * T;
-                const uint2 m = *pp;
-                *pp = make_uint2(max(m.x, key), max(m.y, min(m.x, key)));
-            } else if (code == kCodeGeneral) {
-                const float d = desc_delay(n, rv, n.comp[cc].loc_begin + (b & 31u), x);
-                const unsigned long long key =
-                    (static_cast<unsigned long long>(delay_key(d)) << 32) | bitrev_bits(cc, bits);
-                if (key < best) {
-                    best = key;
-                    bestd = d;
-                }
-            }
-        }
+        const uint32_t wd = rv.lw[q * T], cc = 4u * q;
+        const uint32_t rq = hi_shift ? (__brev(q) >> (32u - hi_shift)) : 0u;
+        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, rq, best, bestd);
+        race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, rq + (2u << hi_shift), best, bestd);
+        race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, rq + (1u << hi_shift), best, bestd);
+        race_member<ALLCLS, 3>(n, bits, rv, wd, cc + 3u, blk.w, rq + (3u << hi_shift), best, bestd);
     }
-    uint32_t inf_classes = 0;
-    for (uint32_t g = 0; g < NG; ++g) {
-        uint32_t a, second;
-        merge_chains(rv.keys[(4u * g) * T], rv.keys[(4u * g + 1u) * T], rv.keys[(4u * g + 2u) * T],
-                     rv.keys[(4u * g + 3u) * T], a, second);
+    if (C & 3u) {  // the last, partly filled word
+        const u32x4 blk = philox_block(K, ps, Qf);
+        const uint32_t wd = rv.lw[Qf * T], cc = 4u * Qf, rem = C & 3u;
+        const uint32_t rq = hi_shift ? (__brev(Qf) >> (32u - hi_shift)) : 0u;
+        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, rq, best, bestd);
+        if (rem > 1u) race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, rq + (2u << hi_shift), best, bestd);
+        if (rem > 2u) race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, rq + (1u << hi_shift), best, bestd);
+    }
+    // each class races with its largest key
+    uint32_t inf_classes = 0, ties = 0;
+    uint32_t top[CSMC_RACE_CLASSES];
+    float dcls[CSMC_RACE_CLASSES], icls[CSMC_RACE_CLASSES];
+#pragma unroll
+    for (uint32_t g = 0; g < CSMC_RACE_CLASSES; ++g) {
+        top[g] = 0u;
+        dcls[g] = 0.0f;
+        icls[g] = 0.0f;
+        if (g >= NG) continue;
+        const uint32_t *kg = rv.keys + (4u * g) * T;
+        const uint32_t a = max(max(kg[0], kg[T]), max(kg[2u * T], kg[3u * T]));
         // key 0 (draw 0 at bit-reversed index 255) is also the "no member"
         // value; only component 255 of a 256-component network can hold it
         if (a == 0u && !(C == 256u && (rv.byte_of(255u) >> 5) == g)) continue;
-        const uint32_t m1 = a >> 8, br1 = 255u - (a & 255u);
-        const uint32_t li = rv.loc(n, bitrev_bits(br1, bits));
-        const uint64_t dsc = n.loc_desc[li];
-        const uint32_t lo = static_cast<uint32_t>(dsc), fl = static_cast<uint32_t>(dsc >> 32);
-        const float inv = (fl & CSMC_DESC_PROG) ? rv.rates[lo] : __uint_as_float(lo);
+        const uint32_t sg = src[g];
+        const float inv = (sg & CSMC_CLASS_SRC_PROG) ? rv.rates[sg & 0xffffu] : __uint_as_float(sg);
         if (!(inv > 0.0f)) return false;  // delays 0, negative or NaN for the whole class
         if (!(inv <= 3.40282347e38f)) {   // +inf: the class's delays are +inf (NaN at u = 1)
             inf_classes |= 1u << g;
             continue;
         }
+        const uint32_t m1 = a >> 8, br1 = 255u - (a & 255u);
         const float d1 = exp_delay(m1 << 8, inv);
-        if (m1 > 0 && second != 0u && exp_delay((m1 - 1u) << 8, inv) == d1) {
-            const uint32_t m2 = second >> 8;
-            if (m2 == m1 || exp_delay(m2 << 8, inv) == d1) return false;
-        }
+        top[g] = a;
+        dcls[g] = d1;
+        icls[g] = inv;
+        ties |= m1 > 0u ? (1u << g) : 0u;
         const unsigned long long key = (static_cast<unsigned long long>(delay_key(d1)) << 32) | br1;
         if (key < best) {
             best = key;
             bestd = d1;
         }
+    }
+    // a class can hide a tie (a lower draw of a member with a smaller index
+    // that rounds to the same delay) only when its delay is the race's
+    // minimum and its largest draw sits on a flat spot of the delay; the
+    // exact race decides those steps
+#pragma unroll
+    for (uint32_t g = 0; g < CSMC_RACE_CLASSES; ++g) {
+        if (!((ties >> g) & 1u) || dcls[g] != bestd) continue;
+        if (exp_delay(((top[g] >> 8) - 1u) << 8, icls[g]) == dcls[g]) return false;
     }
     if (inf_classes && static_cast<uint32_t>(best >> 32) >= delay_key(__uint_as_float(0x7f800000u))) return false;
     return true;
@@ -173,13 +210,14 @@ static __device__ __forceinline__ bool race_coded(const Net &n, uint32_t C, uint
 #define CSMC_CODED_MIN_CTAS_PER_SM 4
 #endif
 
-template <bool VERIFY, bool SLOTS>
+template <bool VERIFY, bool SLOTS, bool ALLCLS>
 __global__ void __launch_bounds__(128, CSMC_CODED_MIN_CTAS_PER_SM) coded_kernel(const __grid_constant__ SimParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     stage_network(smem, p.blob, p.blob_bytes);
     const uint32_t C = p.net.n_comps, V = p.net.n_vars, P = p.net.n_rate_prog;
     const uint32_t T = blockDim.x, t = threadIdx.x;
-    const CodedView rv = carve_coded_view(smem + p.blob_bytes, V, P, C, T, t);
+    const bool recv = (p.net.recv_lo | p.net.recv_hi) != 0;
+    const CodedView rv = carve_coded_view(smem + p.blob_bytes, V, P, C, p.net.n_classes, recv, T, t);
     // padding bytes of the last location word never change
     if (C & 3u) rv.lw[(C >> 2) * T] = kCodePad * 0x20202020u;  // 0xc0 in every byte
     __syncthreads();
@@ -248,7 +286,7 @@ __global__ void __launch_bounds__(128, CSMC_CODED_MIN_CTAS_PER_SM) coded_kernel(
         }
         unsigned long long best;
         float bestd;
-        if (!race_coded(n, C, bits, NG, rv, p.keys, run, step, best, bestd))
+        if (!race_coded<ALLCLS>(n, C, bits, NG, rv, p.keys, p.class_src, run, step, best, bestd))
             race_exact(n, C, bits, rv, p.seed, run, step, best, bestd);
         const uint32_t win = bitrev_bits(static_cast<uint32_t>(best & 0xffffffffull), bits);
         if (run_commit<VERIFY, SLOTS>(n, p.net.n_clocks, rv, sc, p.seed, p.var_id, run, step, time, win, bestd))
@@ -261,18 +299,18 @@ __global__ void __launch_bounds__(128, CSMC_CODED_MIN_CTAS_PER_SM) coded_kernel(
 
 }  // namespace detail
 
-template <bool VERIFY, bool SLOTS>
+template <bool VERIFY, bool SLOTS, bool ALLCLS>
 int coded_launch_one(const SimParams &p, int grid, int block, size_t smem, void *stream) {
-    auto fn = detail::coded_kernel<VERIFY, SLOTS>;
+    auto fn = detail::coded_kernel<VERIFY, SLOTS, ALLCLS>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     fn<<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return static_cast<int>(cudaGetLastError());
 }
 
-template <bool VERIFY, bool SLOTS>
+template <bool VERIFY, bool SLOTS, bool ALLCLS>
 int coded_occupancy_one(int block, size_t smem, int *ctas) {
-    auto fn = detail::coded_kernel<VERIFY, SLOTS>;
+    auto fn = detail::coded_kernel<VERIFY, SLOTS, ALLCLS>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     return static_cast<int>(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, smem));

@@ -29,6 +29,7 @@ struct Net {
     const uint32_t *rate_prog;
     const uint16_t *clock;
     const uint64_t *loc_desc;
+    const uint32_t *loc_inv1;  // CSMC_DESC_INV1 locations' invariant (null in blobs without the table)
     uint32_t n_comps, n_vars, n_rate_prog, flags, n_clocks, recv_lo, recv_hi;
 };
 
@@ -48,6 +49,7 @@ static __device__ __forceinline__ Net net_view(const uint8_t *base) {
     n.rate_prog = reinterpret_cast<const uint32_t *>(base + h->off_rate_prog);
     n.clock = reinterpret_cast<const uint16_t *>(base + h->off_clock);
     n.loc_desc = reinterpret_cast<const uint64_t *>(base + h->off_loc_desc);
+    n.loc_inv1 = h->off_loc_inv1 ? reinterpret_cast<const uint32_t *>(base + h->off_loc_inv1) : nullptr;
     n.n_comps = h->n_comps;
     n.n_vars = h->n_vars;
     n.n_rate_prog = h->n_rate_prog;
@@ -74,6 +76,7 @@ static __device__ __forceinline__ Net net_view(const uint8_t *base, const NetLay
     n.rate_prog = reinterpret_cast<const uint32_t *>(base + l.off_rate_prog);
     n.clock = reinterpret_cast<const uint16_t *>(base + l.off_clock);
     n.loc_desc = reinterpret_cast<const uint64_t *>(base + l.off_loc_desc);
+    n.loc_inv1 = l.off_loc_inv1 ? reinterpret_cast<const uint32_t *>(base + l.off_loc_inv1) : nullptr;
     n.n_comps = l.n_comps;
     n.n_vars = l.n_vars;
     n.n_rate_prog = l.n_rate_prog;
@@ -184,11 +187,34 @@ static __device__ __noinline__ double eval_prog(const Net &n, VarView vars, uint
     }
 }
 
-// Any expression handle: literals and variables inline, programs out of line.
+// Operand of a PUSH_C / PUSH_V instruction.
+static __device__ __forceinline__ double chain_operand(const Net &n, VarView vars, uint64_t ins) {
+    const uint32_t a = CSMC_INS_A(ins);
+    return CSMC_INS_OP(ins) == CSMC_OP_PUSH_V ? static_cast<double>(vars[a]) : n.konst[a];
+}
+
+// v1 op v2 for the operators of CSMC_PROG_CHAIN programs (apply_op's
+// arithmetic for them).
+static __device__ __forceinline__ double chain_op(uint32_t op, double v1, double v2) {
+    if (op == CSMC_OP_ADD || op == CSMC_OP_TADD) return d_add(v1, v2);
+    if (op == CSMC_OP_SUB || op == CSMC_OP_TSUB) return d_sub(v1, v2);
+    if (op == CSMC_OP_MUL || op == CSMC_OP_TMUL) return d_mul(v1, v2);
+    return d_div(v1, v2);
+}
+
+// Any expression handle: literals and variables inline, programs of one or
+// two binary operations (CSMC_PROG_CHAIN) inline, others out of line.
 static __device__ __forceinline__ double eval(const Net &n, VarView vars, uint32_t h) {
     const uint32_t tag = CSMC_H_TAG(h), p = CSMC_H_PAYLOAD(h);
     if (tag == CSMC_H_LIT) return n.konst[p];
     if (tag == CSMC_H_VAR) return static_cast<double>(vars[p]);
+    if (CSMC_INS_A(n.code[p]) & CSMC_PROG_CHAIN) {
+        double r = chain_op(CSMC_INS_OP(n.code[p + 3]), chain_operand(n, vars, n.code[p + 1]),
+                            chain_operand(n, vars, n.code[p + 2]));
+        const uint64_t i4 = n.code[p + 4];
+        if (CSMC_INS_OP(i4) != CSMC_OP_END) r = chain_op(CSMC_INS_OP(n.code[p + 5]), r, chain_operand(n, vars, i4));
+        return r;
+    }
     return eval_prog(n, vars, p);
 }
 
@@ -250,6 +276,18 @@ static __device__ __forceinline__ float comp_delay(const Net &n, VarView vars, V
         inv = inv_rate(eval(n, vars, L.rate));
     }
     return exp_delay(x, inv);
+}
+
+// Delay of a CSMC_DESC_INV1 location (comp_delay's arithmetic for one
+// invariant clock <= / < literal): uniform on (0, bound - clock] while the
+// bound lies ahead, else exponential with the descriptor's 1/rate.
+static __device__ __forceinline__ float inv1_delay(const Net &n, VarView vars, VarView rates, uint32_t li,
+                                                   uint32_t lo, uint32_t fl, uint32_t x) {
+    const uint32_t w = n.loc_inv1[li];
+    double ttb = d_sub(n.konst[CSMC_INV1_CONST(w)], static_cast<double>(vars[CSMC_INV1_VAR(w)]));
+    if (CSMC_INV1_STRICT(w)) ttb = d_sub(ttb, 1e-6);
+    if (ttb >= 0) return uniform_delay(x, ttb);
+    return exp_delay(x, (fl & CSMC_DESC_PROG) ? rates[lo] : __uint_as_float(lo));
 }
 
 // Enabled-edge slot state after writing the enabled list `en` (ascending):

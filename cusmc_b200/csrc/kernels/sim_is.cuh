@@ -345,7 +345,6 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
     const uint32_t C = p.net.n_comps, V = p.net.n_vars, P = p.net.n_rate_prog;
     const bool rate_table = (p.net.flags & CSMC_NET_RATE_TABLE) && P > 0;
     const uint32_t bits = ceil_log2(C);
-    const uint32_t n_int = V < 4 ? V : 4;
     const uint32_t lane = threadIdx.x & 31u;
     uint8_t *slab = smem + p.blob_bytes + sizeof(MlpSmem) + static_cast<size_t>(threadIdx.x >> 5) * ip.slab_bytes;
     float *h1s = reinterpret_cast<float *>(slab);
@@ -357,7 +356,7 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
     // theta is a function of the shared features x[4..15] alone (the network
     // is fixed for the launch): the last evaluated features and their class
     // factors, kept across steps and runs (steps that change no variable
-    // and stay within one BF16 step of t / T reuse them)
+    // and stay within one 1/64 step of t / T reuse them)
     uint32_t x_last[CSMC_MLP_IN - 4];
 #pragma unroll
     for (int i = 0; i < CSMC_MLP_IN - 4; ++i) x_last[i] = 0xffffffffu;  // a NaN: never equal to a feature
@@ -434,10 +433,14 @@ __global__ void __launch_bounds__(CSMC_IS_BLOCK, CSMC_IS_MIN_CTAS_PER_SM) is_war
             }
 
             // the proposal's class factors
+            const MlpFeatures &F = ip.feat;
             float v4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            for (uint32_t i = 0; i < n_int; ++i) v4[i] = rv.vars[i];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (F.var[i] >= 0) v4[i] = rv.vars[F.var[i]];
+            const float clk = F.clock_var >= 0 ? rv.vars[F.clock_var] : 0.0f;
             float x[CSMC_MLP_IN];
-            mlp_features(0, v4, n_int, C, time, p.horizon, x);
+            mlp_features(0, F, v4, clk, time, p.horizon, x);
             bool same = true;
 #pragma unroll
             for (int i = 4; i < CSMC_MLP_IN; ++i) same = same && (__float_as_uint(x[i]) == x_last[i - 4]);

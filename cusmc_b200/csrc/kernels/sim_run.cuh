@@ -17,9 +17,12 @@
 namespace csmc {
 namespace detail {
 
-// Delay of a component whose location is invariant-bounded, or whose rate
-// is evaluated per component (uncommon; out of line).
-static __device__ __noinline__ float slow_delay(const Net &n, VarView vars, VarView rates, uint32_t li, uint32_t x) {
+// Delay of a component whose descriptor flags INV or EVAL: the one-
+// invariant form inline here, the rest through comp_delay.  One call site
+// per component keeps the race loops' register budget.
+static __device__ __noinline__ float bounded_delay(const Net &n, VarView vars, VarView rates, uint32_t li,
+                                                   uint32_t lo, uint32_t fl, uint32_t x) {
+    if (fl & CSMC_DESC_INV1) return inv1_delay(n, vars, rates, li, lo, fl, x);
     return comp_delay(n, vars, rates, li, x);
 }
 
@@ -227,7 +230,7 @@ static __device__ __forceinline__ void race_exact(const Net &n, uint32_t C, uint
                 if (fl & CSMC_DESC_PROG) inv = rv.rates[lo];
                 float d = exp_delay(x, inv);
                 if (fl & (CSMC_DESC_ZERO | CSMC_DESC_INV | CSMC_DESC_EVAL))
-                    d = (fl & CSMC_DESC_ZERO) ? 0.0f : slow_delay(n, rv.vars, rv.rates, li, x);
+                    d = (fl & CSMC_DESC_ZERO) ? 0.0f : bounded_delay(n, rv.vars, rv.rates, li, lo, fl, x);
                 const unsigned long long key =
                     (static_cast<unsigned long long>(delay_key(d)) << 32) | bitrev_bits(cc, bits);
                 if (key < best) {
@@ -287,7 +290,7 @@ static __device__ __forceinline__ bool race_classes(const Net &n, uint32_t C, ui
                     if (fl & CSMC_DESC_ZERO) {
                         d = 0.0f;
                     } else if (fl & (CSMC_DESC_INV | CSMC_DESC_EVAL)) {
-                        d = slow_delay(n, rv.vars, rv.rates, li, x);
+                        d = bounded_delay(n, rv.vars, rv.rates, li, lo, fl, x);
                     } else {
                         const float inv = (fl & CSMC_DESC_PROG) ? rv.rates[lo] : __uint_as_float(lo);
                         d = exp_delay(x, inv);

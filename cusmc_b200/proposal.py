@@ -124,6 +124,33 @@ def set_inference(net, tensor_cores: bool) -> None:
     check(lib().csmc_is_set_inference(net._h, 1 if tensor_cores else 0))
 
 
+def set_kernel(net, family: int) -> None:
+    """Kernel of runs under the proposal: 0 = one thread per run where the
+    network qualifies (else one warp per run), 3 = always one warp per run.
+    Both give the same runs bit for bit."""
+    check(lib().csmc_is_set_kernel(net._h, family))
+
+
+def set_features(net, count_vars=None, scales=None, clock_var: int = -1) -> None:
+    """The network's feature source (csmc_is_set_features): count_vars (4
+    variable ids, -1 unused) feed features 5..8 times scales; clock_var
+    feeds feature 4.  No arguments: the default (variables 0..3 over the
+    component count, no clock)."""
+    cv = None if count_vars is None else (ctypes.c_int32 * 4)(*count_vars)
+    sc = None if scales is None else (ctypes.c_float * 4)(*scales)
+    check(lib().csmc_is_set_features(net._h, cv, sc, int(clock_var)))
+
+
+def pack_features(n_vars: int, n_comps: int, count_vars=None, scales=None, clock_var: int = -1) -> bytes:
+    """The same feature source packed as csmc::MlpFeatures (for the CPU
+    oracle's is_run / is_trace)."""
+    var = list(count_vars) if count_vars is not None else [i if i < n_vars else -1 for i in range(4)]
+    inv_c = np.float32(1.0) / np.float32(n_comps)
+    sc = list(scales) if scales is not None else [inv_c] * 4
+    return (np.array(var, np.int32).tobytes() + np.array(sc, np.float32).tobytes() +
+            np.array([clock_var, 0, 0, 0], np.int32).tobytes())
+
+
 def is_run(net, query: Query, params: bytes, seed: int, n_runs: int, first_run: int = 0, flags=None, logw=None,
            values=None, steps=None, stream=None) -> Result:
     """csmc_is_run on a Network; per-run outputs are optional torch CUDA tensors."""

@@ -74,7 +74,8 @@ typedef struct {
     int32_t runs_per_cta;   /* runs in flight per CTA */
     int32_t family;         /* 0 lane-group kernel, 1 thread-per-run kernel, 2 thread-per-run with
                                the network in global memory (batch kernel, one job), 3 importance
-                               sampling (one warp per run), 4 class-coded thread-per-run kernel */
+                               sampling (one warp per run), 4 class-coded thread-per-run kernel,
+                               5 importance sampling (one thread per run, tilt groups) */
 } csmc_result;
 
 /* Thread-local message of the last failure on this thread. */
@@ -209,6 +210,15 @@ int csmc_batch_create(csmc_net *const *nets, const csmc_query *qs, const uint64_
 int csmc_batch_set_plan(csmc_batch *b, int32_t threads_per_cta, int32_t ctas_per_sm);
 int csmc_batch_plan(const csmc_batch *b, int32_t *threads_per_cta, int32_t *ctas_per_sm);
 
+/* Jobs whose networks have min_comps .. 512 components are simulated one
+ * warp per run (32 lanes, up to 16 components each) instead of one thread
+ * per run; every warp takes those runs first, then joins the one-thread-per-
+ * run queue.  0: every job runs one thread per run.  Default 128.  The
+ * per-run results do not depend on it.  csmc_batch_group_comps reports the
+ * threshold and how many jobs it selects. */
+int csmc_batch_set_group_comps(csmc_batch *b, int32_t min_comps);
+int csmc_batch_group_comps(const csmc_batch *b, int32_t *min_comps, int32_t *group_jobs);
+
 /* Enqueues the whole batch on stream — counter reset, the simulation, the
  * per-job value sums and the copies of the counters and sums into the
  * batch's pinned host buffers — without allocating or synchronising, so the
@@ -237,9 +247,12 @@ int csmc_batch_outputs_host(const csmc_batch *b, int32_t job, uint8_t *flags, do
 /* Autotuner for the batch: runs a probe batch (each job's runs scaled by
  * probe_fraction, at least one run, every run capped at 2000 race steps) at
  * each candidate geometry (64 and 128 threads per CTA, every CTAs-per-SM
- * count that fits), keeps the fastest, and orders the jobs in the run space
- * by measured cost per run (where no probe run reached the cap), most
- * expensive first, so that the cheapest runs fill the end of the batch. */
+ * count that fits), keeps the fastest, then at that geometry tries the
+ * warp-per-run thresholds 0, 64, 128 and 256 components
+ * (csmc_batch_set_group_comps) and keeps the fastest; it orders the jobs of
+ * each run space by measured cost per run (where no probe run reached the
+ * cap), most expensive first, so that the cheapest runs fill the end of the
+ * batch. */
 int csmc_batch_autotune(csmc_batch *b, double probe_fraction, int32_t *threads_per_cta, int32_t *ctas_per_sm);
 
 void csmc_batch_free(csmc_batch *b);
@@ -258,6 +271,23 @@ void csmc_batch_free(csmc_batch *b);
  * CUDA-core evaluation is the faster one.  Weights and estimates are exact
  * for the theta a run used either way. */
 int csmc_is_set_inference(csmc_net *net, int32_t tensor_cores);
+
+/* Which kernel simulates runs under the proposal (csmc_is_run; replay
+ * always runs one warp per run).  0 (default): one thread per run (result
+ * family 5) when the network has race classes (at most 256 components, 32
+ * locations per automaton), theta is evaluated on CUDA cores and the state
+ * fits, else one warp per run (family 3); 3: always one warp per run.  The
+ * runs, paths and log-likelihood ratios are the same bits either way. */
+int csmc_is_set_kernel(csmc_net *net, int32_t family);
+
+/* Where the proposal's features come from for this network (default:
+ * count_vars = variables 0..3, scales = 1 / components, no clock):
+ * count_vars[4] (variable ids, -1 unused) feed features 5..8 as value *
+ * scales[i]; clock_var (-1: none) feeds feature 4 as its value / T, rounded
+ * down to a multiple of 1/64.  NULL arrays keep the default for that part;
+ * all three defaults restore the default source.  The epidemic's default
+ * (its S, E, I, R counts over N) is the first form. */
+int csmc_is_set_features(csmc_net *net, const int32_t *count_vars, const float *scales, int32_t clock_var);
 
 /* Runs first_run .. first_run+n_runs-1 under the proposal.  Per-run device
  * outputs (may be NULL): flags, logw (log-likelihood ratio nominal/proposal,

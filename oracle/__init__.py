@@ -38,13 +38,13 @@ def lib():
                                    ctypes.POINTER(ctypes.c_size_t)]
         h.oracle_is_run.restype = ctypes.c_int
         h.oracle_is_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(Query), ctypes.c_char_p,
-                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
-                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.POINTER(ctypes.c_double)]
         h.oracle_is_trace.restype = ctypes.c_int
         h.oracle_is_trace.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(Query), ctypes.c_char_p,
-                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
-                                      ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                      ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
                                       ctypes.POINTER(ctypes.c_uint64)]
         h.oracle_mlp_theta.restype = ctypes.c_float
         h.oracle_mlp_theta.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
@@ -90,15 +90,18 @@ def run(blob: bytes, query: Query, seed: int, n_runs: int, first_run: int = 0, t
 ROW_DTYPE = np.dtype([("x", "<u2", (16,)), ("a", "<f4"), ("b", "<f4")])  # csmc::MlpRow, 40 bytes
 
 
-def is_run(blob: bytes, query: Query, params: bytes, seed: int, n_runs: int, first_run: int = 0, threads: int = 0):
+def is_run(blob: bytes, query: Query, params: bytes, seed: int, n_runs: int, first_run: int = 0, threads: int = 0,
+           features: bytes | None = None):
     """Runs under the proposal network on the host: dict of per-run flags,
-    logw, values, steps; wall milliseconds."""
+    logw, values, steps; wall milliseconds.  features: a packed feature
+    source (cusmc_b200.proposal.pack_features), None for the default."""
     flags = np.zeros(n_runs, dtype=np.uint8)
     logw = np.zeros(n_runs, dtype=np.float64)
     values = np.zeros(n_runs, dtype=np.float64)
     steps = np.zeros(n_runs, dtype=np.uint32)
     ms = ctypes.c_double()
-    rc = lib().oracle_is_run(blob, len(blob), ctypes.byref(query), params, seed & (2**64 - 1), first_run, n_runs,
+    rc = lib().oracle_is_run(blob, len(blob), ctypes.byref(query), params, features, seed & (2**64 - 1), first_run,
+                             n_runs,
                              threads, flags.ctypes.data, logw.ctypes.data, values.ctypes.data, steps.ctypes.data,
                              ctypes.byref(ms))
     if rc != 0:
@@ -107,13 +110,13 @@ def is_run(blob: bytes, query: Query, params: bytes, seed: int, n_runs: int, fir
 
 
 def is_trace(blob: bytes, query: Query, params: bytes, seed: int, runs, weights, first_run: int = 0,
-             cap: int = 1 << 22) -> np.ndarray:
+             cap: int = 1 << 22, features: bytes | None = None) -> np.ndarray:
     """Training rows of the listed runs (four per step, run-list order)."""
     runs = np.ascontiguousarray(runs, dtype=np.uint64)
     weights = np.ascontiguousarray(weights, dtype=np.float32)
     rows = np.zeros(cap, dtype=ROW_DTYPE)
     n = ctypes.c_uint64()
-    rc = lib().oracle_is_trace(blob, len(blob), ctypes.byref(query), params, seed & (2**64 - 1), first_run,
+    rc = lib().oracle_is_trace(blob, len(blob), ctypes.byref(query), params, features, seed & (2**64 - 1), first_run,
                                runs.ctypes.data, weights.ctypes.data, len(runs), rows.ctypes.data, cap,
                                ctypes.byref(n))
     if rc != 0:

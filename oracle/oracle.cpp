@@ -344,9 +344,11 @@ class Run {
             float feat[CSMC_MLP_CLASSES][CSMC_MLP_IN];
             if (mlp_) {  // the proposal's class factors for this step
                 float v4[4] = {0, 0, 0, 0};
-                for (uint32_t i = 0; i < 4 && i < V; ++i) v4[i] = vars_[i];
+                for (int i = 0; i < 4; ++i)
+                    if (feat_.var[i] >= 0) v4[i] = vars_[feat_.var[i]];
+                const float clk = feat_.clock_var >= 0 ? vars_[feat_.clock_var] : 0.0f;
                 for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) {
-                    mlp_features(l, v4, V < 4 ? V : 4, C, time, T, feat[l]);
+                    mlp_features(l, feat_, v4, clk, time, T, feat[l]);
                     mfac[l] = tilt_factor(mlp_theta(*mlp_, feat[l]));
                 }
             }
@@ -427,6 +429,7 @@ class Run {
     }
 
     const MlpParams *mlp_ = nullptr;   // importance sampling: the proposal network
+    MlpFeatures feat_{};                // importance sampling: where its features come from
     double logw_ = 0.0;                 // log-likelihood ratio of the path
     std::vector<MlpRow> *rows_ = nullptr;  // replay: training rows
     float row_w_ = 0.0f;                // replay: the run's CE weight
@@ -634,16 +637,28 @@ int oracle_trace(const void *blob, size_t bytes, const csmc_query *q, uint64_t s
     }
 }
 
-/* Importance sampling under the proposal network P (host MlpParams):
- * per run (host, may be NULL): flags, log-likelihood ratios (nominal over
- * proposal), tracked values, steps.  Threads as oracle_run. */
-int oracle_is_run(const void *blob, size_t bytes, const csmc_query *q, const void *params, uint64_t seed,
-                  uint64_t first_run, uint64_t n_runs, int threads, uint8_t *flags, double *logw, double *values,
-                  uint32_t *steps, double *wall_ms) {
+// The feature source of a run: features (may be NULL: the default of the network).
+static MlpFeatures features_of(const Net &n, const void *features) {
+    if (features) {
+        MlpFeatures F;
+        std::memcpy(&F, features, sizeof F);
+        return F;
+    }
+    return mlp_default_features(n.h->n_vars, n.h->n_comps);
+}
+
+/* Importance sampling under the proposal network P (host MlpParams) with
+ * the feature source features (csmc::MlpFeatures, may be NULL: the
+ * default): per run (host, may be NULL): flags, log-likelihood ratios
+ * (nominal over proposal), tracked values, steps.  Threads as oracle_run. */
+int oracle_is_run(const void *blob, size_t bytes, const csmc_query *q, const void *params, const void *features,
+                  uint64_t seed, uint64_t first_run, uint64_t n_runs, int threads, uint8_t *flags, double *logw,
+                  double *values, uint32_t *steps, double *wall_ms) {
     try {
         if (!q || !params) throw std::runtime_error("null argument");
         const Net n = view(blob, bytes);
         const MlpParams *P = static_cast<const MlpParams *>(params);
+        const MlpFeatures F = features_of(n, features);
         int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
         if (nt < 1) nt = 1;
         if (static_cast<uint64_t>(nt) > n_runs) nt = static_cast<int>(std::max<uint64_t>(1, n_runs));
@@ -654,6 +669,7 @@ int oracle_is_run(const void *blob, size_t bytes, const csmc_query *q, const voi
                 if (i >= n_runs) break;
                 Run r(n, *q, seed, first_run + i);
                 r.mlp_ = P;
+                r.feat_ = F;
                 r.simulate(false);
                 const double val = q->is_max ? r.qmax_ : r.qmin_;
                 uint8_t f = r.flag_;
@@ -681,16 +697,18 @@ int oracle_is_run(const void *blob, size_t bytes, const csmc_query *q, const voi
 /* Replays runs first_run + runs[i] under P and appends their training rows
  * (weighted by weights[i]) in run-list order to rows (capacity cap rows);
  * *n_rows receives the number written (CSMC_ERR_LIMIT when cap is short). */
-int oracle_is_trace(const void *blob, size_t bytes, const csmc_query *q, const void *params, uint64_t seed,
-                    uint64_t first_run, const uint64_t *runs, const float *weights, uint64_t n_list, void *rows,
-                    uint64_t cap, uint64_t *n_rows) {
+int oracle_is_trace(const void *blob, size_t bytes, const csmc_query *q, const void *params, const void *features,
+                    uint64_t seed, uint64_t first_run, const uint64_t *runs, const float *weights, uint64_t n_list,
+                    void *rows, uint64_t cap, uint64_t *n_rows) {
     try {
         const Net n = view(blob, bytes);
         const MlpParams *P = static_cast<const MlpParams *>(params);
+        const MlpFeatures F = features_of(n, features);
         std::vector<MlpRow> out;
         for (uint64_t i = 0; i < n_list; ++i) {
             Run r(n, *q, seed, first_run + runs[i]);
             r.mlp_ = P;
+            r.feat_ = F;
             r.rows_ = &out;
             r.row_w_ = weights[i];
             r.simulate(false);

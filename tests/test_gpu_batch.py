@@ -68,11 +68,19 @@ def _assert_job_equal(batch_res, batch_out, single_res, single_out):
     assert batch_res.estimate == single_res.estimate
 
 
-def test_batch_matches_single_network_runs():
+@pytest.mark.parametrize("group_comps", [None, 0, 2, 64])
+def test_batch_matches_single_network_runs(group_comps):
+    """group_comps: the warp-per-run threshold (None: the default, 128; 0:
+    every job one thread per run; 2: every job one warp per run)."""
     jobs = _jobs()
     singles = [_single(*j) for j in jobs]
     batch = api.Batch(jobs, verify=True)
     try:
+        if group_comps is not None:
+            batch.set_group_comps(group_comps)
+        expect = sum(1 for j in jobs
+                     if group_comps != 0 and (group_comps or 128) <= j[0].info["n_comps"] <= 512)
+        assert batch.group_comps()[1] == expect
         for use_graph in (False, True, True):  # direct, graph capture, graph replay
             res = batch.run(use_graph=use_graph)
             for i, j in enumerate(jobs):
@@ -83,7 +91,38 @@ def test_batch_matches_single_network_runs():
             j[0].close()
 
 
-def test_batch_job_against_the_oracle():
+def test_large_networks_one_warp_per_run_match_single_runs():
+    """Networks of 130, 230 and 303 components (4, 8 and 16 components per
+    lane in warp-per-run mode) beside small ones, against csmc_run_verify."""
+    big = netgen.batch_networks(count=54, base_seed=1000)
+    specs = [(big[53], 48), (big[7], 40), (big[13], 24), (netgen.mutex(8), 500), (netgen.random_network(0), 700)]
+    jobs = []
+    for i, (w, runs) in enumerate(specs):
+        net = api.Network(_blob(w))
+        q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
+        jobs.append((net, q, 9100 + i, runs, 5 * i))
+    singles = [_single(*j) for j in jobs]
+    try:
+        for k_expect, thr in ((16, 128), (16, 2)):
+            batch = api.Batch(jobs, verify=True)
+            try:
+                batch.set_group_comps(thr)
+                res = batch.run(use_graph=True)
+                for i in range(len(jobs)):
+                    _assert_job_equal(res[i], batch.outputs(i), *singles[i])
+                    in_group = jobs[i][0].info["n_comps"] >= thr
+                    assert res[i].lanes_per_run == (32 if in_group else 1)
+                    if in_group:
+                        assert res[i].comps_per_lane == k_expect
+            finally:
+                batch.close()
+    finally:
+        for j in jobs:
+            j[0].close()
+
+
+@pytest.mark.parametrize("group_comps", [0, 2])
+def test_batch_job_against_the_oracle(group_comps):
     import oracle
     w = netgen.random_network(3)
     blob = _blob(w)
@@ -93,6 +132,7 @@ def test_batch_job_against_the_oracle():
     q2 = api.variable_query(1, 200, threshold=1, is_max=True)
     batch = api.Batch([(other, q2, 5, 2000), (net, q, 11, 1500, 200)], verify=True)
     try:
+        batch.set_group_comps(group_comps)
         res = batch.run(use_graph=True)
         out = batch.outputs(1)
         r_cpu, cpu, _ = oracle.run(blob, q, 11, 1500, 200, threads=0, digests=True, final_state=True)

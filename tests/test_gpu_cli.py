@@ -65,3 +65,32 @@ def test_formula_json_and_run_dump_match_the_library(tmp_path):
     r, flags, values, _ = api.run_host(blob, q, 11, 3000)
     assert d["result"] == pytest.approx(r.hits / 3000, abs=0)
     assert np.array_equal(table["value"], values)
+
+
+def test_importance_sampling_from_the_command_line(tmp_path):
+    """--csmc-is: CE training through the C ABI, then weighted runs; the
+    estimate agrees with plain SMC on an event that plain SMC sees often."""
+    w = netgen.epidemic(n_agents=30)
+    model = w.write(str(tmp_path / "epi.xml"))
+    run = tmp_path / "run"
+    run.mkdir()
+    js = tmp_path / "is.json"
+    p = _run(["-m", model, "-s", "3", "-q", "20000", "60", "9", "3", "1", "0", "", "--csmc-is",
+              "--csmc-is-ce", "3,3000,5,0.03", "--csmc-json", str(js)], run)
+    assert p.returncode == 1, p.stderr
+    assert "Importance sampling: learned proposal, up to 3 CE rounds of 3000 runs" in p.stdout
+    assert re.search(r"^CE round 0: level ", p.stdout, re.M)
+    out = json.load(open(js))
+    assert out["method"].startswith("importance sampling") and out["simulations"] == 20000
+    lo, hi = out["ci95"]
+    blob = api.compile_model(model)
+    net = api.Network(blob)
+    try:
+        r = net.run(api.variable_query(3, 60, threshold=9, is_max=True), 77, 400_000)
+    finally:
+        net.close()
+    half_plain = 1.96 * np.sqrt(r.estimate * (1 - r.estimate) / 400_000)
+    assert lo - half_plain <= r.estimate <= hi + half_plain
+    # an estimate query (IS_ESTIMATE = 1) has no probability to sample: refused with an error
+    p = _run(["-m", model, "-q", "1000", "60", "9", "3", "1", "1", "", "--csmc-is"], run)
+    assert "Error:" in p.stderr

@@ -3,15 +3,18 @@ model file and query: the stdout report must be the same line for line
 (main.cu:39-110, smc.cu:317,358-372,402, simulation/statistics.cuh:126-169),
 except for the run-dependent numbers in the result and timing lines, and
 the ../results5.csv each program writes must have the same header row and
-row keys (simulation/write_csv.cu:15-98).  The two estimates must also agree
-within Chernoff-Hoeffding bounds.
+row keys (simulation/write_csv.cu:15-98).  The estimates are not compared
+here: the reference's runs share one array of curand states across all
+concurrently running blocks (USE_GLOBAL_MEMORY_CURAND, smc.cu:227-237,
+simulation.cu:691-760), so its runs are not independent and a binomial
+bound on a few thousand runs does not hold for it; the estimates are pinned
+at large run counts by test_ref_estimates.py.
 
 The reference binaries are built from the reference sources by
 oracle/ref/Makefile (oracle/_ref/cusmc_ref_v<N>, MAX_VARIABLES = N); the
 test is skipped where they were not built.
 """
 import csv
-import math
 import os
 import re
 import subprocess
@@ -82,12 +85,4 @@ def test_cli_report_and_csv_match_the_reference_binary(tmp_path, name, make, qar
     assert rows_o[0] == rows_r[0]
     assert [r[0] for r in rows_o] == [r[0] for r in rows_r]
     assert [len(r) for r in rows_o] == [len(r) for r in rows_r]
-    # the estimates agree within the two Chernoff-Hoeffding bounds (delta 1e-3)
-    n = int(qargs[0])
-    eps = math.sqrt(math.log(2 / 1e-3) / (2 * n))
-    a, b = _result_of(pr.stdout), _result_of(po.stdout)
-    assert a is not None and b is not None
-    if qargs[5] == "1":  # estimate of the mean maximum: scale the bound by the value range
-        assert abs(a - b) <= 2 * eps * 16
-    else:
-        assert abs(a - b) <= 2 * eps
+    assert _result_of(pr.stdout) is not None and _result_of(po.stdout) is not None

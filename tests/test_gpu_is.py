@@ -56,8 +56,14 @@ CASES = {
 }
 
 
+# networks with race classes: csmc_is_run simulates them one thread per run
+# (family 5) unless told to use one warp per run (family 3)
+THREAD_CASES = {"epidemic", "epidemic_160", "mutex"}
+
+
+@pytest.mark.parametrize("kernel", [0, 3])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_is_runs_match_the_oracle(name):
+def test_is_runs_match_the_oracle(name, kernel):
     import torch
     w, T, thr = CASES[name]()
     blob = _blob(w)
@@ -67,6 +73,7 @@ def test_is_runs_match_the_oracle(name):
     n = 512
     net = api.Network(blob)
     P.set_inference(net, False)
+    P.set_kernel(net, kernel)
     try:
         dev = torch.device("cuda")
         flags = torch.zeros(n, dtype=torch.uint8, device=dev)
@@ -76,6 +83,7 @@ def test_is_runs_match_the_oracle(name):
         r = P.is_run(net, q, params, 17, n, 40, flags=flags, logw=logw, values=values, steps=steps)
     finally:
         net.close()
+    assert r.family == (5 if kernel == 0 and name in THREAD_CASES else 3)
     cpu, _ = oracle.is_run(blob, q, params, 17, n, 40)
     assert np.array_equal(flags.cpu().numpy(), cpu["flags"])
     assert np.array_equal(steps.cpu().numpy().view(np.uint32), cpu["steps"])
@@ -234,3 +242,54 @@ def test_c_abi_training_equals_the_python_training():
         assert a["J_start"] == b["j_start"] and a["J_end"] == b["j_end"] and a["hits"] == b["hits"]
     assert prop_c.pack() == P.Proposal.from_vector(prop_c.vector()).pack()
 
+
+
+@pytest.mark.parametrize("case", ["epidemic_permuted", "mutex_clock"])
+def test_feature_source_is_a_network_choice(case):
+    """A non-default feature source (csmc_is_set_features): the epidemic's
+    counts in another order and scale, and a mutex network whose features
+    are its shared variables and one process's clock.  Runs and replay rows
+    stay bit-identical to the oracle given the same source."""
+    import torch
+    if case == "epidemic_permuted":
+        w, T, thr = netgen.epidemic(), 100, 49
+        src = dict(count_vars=[3, 2, 1, 0], scales=[0.02, 0.5 / 100, 0.01, 0.03], clock_var=-1)
+    else:
+        w, T, thr = netgen.mutex(8), None, None
+        src = dict(count_vars=[1, 0, -1, -1], scales=[0.5, 0.125, 1.0, 1.0], clock_var=2)
+    blob = _blob(w)
+    info = api.blob_info(blob)
+    q = api.variable_query(w.var_id, T or w.horizon, threshold=thr if thr is not None else w.threshold,
+                           is_max=True, max_steps=100_000)
+    params = _random_proposal(5).pack()
+    feats = P.pack_features(info["n_vars"], info["n_comps"], **src)
+    n = 384
+    net = api.Network(blob)
+    P.set_inference(net, False)
+    P.set_features(net, **src)
+    try:
+        dev = torch.device("cuda")
+        flags = torch.zeros(n, dtype=torch.uint8, device=dev)
+        logw = torch.zeros(n, dtype=torch.float64, device=dev)
+        steps = torch.zeros(n, dtype=torch.int32, device=dev)
+        P.is_run(net, q, params, 23, n, 7, flags=flags, logw=logw, steps=steps)
+        cpu, _ = oracle.is_run(blob, q, params, 23, n, 7, features=feats)
+        assert np.array_equal(flags.cpu().numpy(), cpu["flags"])
+        assert np.array_equal(steps.cpu().numpy().view(np.uint32), cpu["steps"])
+        assert np.array_equal(logw.cpu().numpy().view(np.uint64), cpu["logw"].view(np.uint64))
+        # the default source gives other paths once theta differs (sanity)
+        cpu_default, _ = oracle.is_run(blob, q, params, 23, n, 7)
+        assert not np.array_equal(cpu_default["logw"], cpu["logw"])
+        # replay rows of a few runs
+        runs = np.arange(0, 16, dtype=np.uint64)
+        wts = np.full(16, 1.0 / 16, np.float32)
+        st = cpu["steps"][:16].astype(np.uint64)
+        offs = np.concatenate([[0], np.cumsum(4 * st)[:-1]]).astype(np.uint64)
+        n_rows = int(4 * st.sum())
+        rows = torch.zeros(n_rows * P.ROW_BYTES, dtype=torch.uint8, device=dev)
+        P.is_trace(net, q, params, 23, torch.from_numpy(runs.view(np.int64)).to(dev), torch.from_numpy(wts).to(dev),
+                   torch.from_numpy(offs.view(np.int64)).to(dev), rows, 7)
+        want = oracle.is_trace(blob, q, params, 23, runs, wts, 7, cap=n_rows, features=feats)
+        assert rows.cpu().numpy().tobytes() == want.tobytes()
+    finally:
+        net.close()

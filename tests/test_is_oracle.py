@@ -112,3 +112,42 @@ def test_gradient_matches_finite_differences():
         _, Jm = oracle.mlp_grad(Proposal.from_vector(vm).pack(), rows)
         fd = (Jp - Jm) / (2 * h)
         assert g[i] == pytest.approx(fd, rel=5e-2, abs=1e-3 * max(1.0, abs(J0))), (i, g[i], fd)
+
+
+def _butterfly(p):
+    """csmc_mlp.h warp_tree_d: offsets 16, 8, 4, 2, 1, lane L adds lane L ^ off."""
+    p = list(p)
+    off = 16
+    while off:
+        p = [p[lane] + p[lane ^ off] for lane in range(32)]
+        off //= 2
+    return p[0]
+
+
+def _bit_reversed_stack(p):
+    """The thread-per-run importance-sampling kernel's order
+    (sim_is_coded.cuh: tree_push): the lanes' partials taken in 5-bit
+    bit-reversed order and merged by a five-level binary-counter stack."""
+    stack = [0.0] * 5
+    for i in range(32):
+        v = p[int(f"{i:05b}"[::-1], 2)]
+        for level in range(5):
+            if not (i >> level) & 1:
+                stack[level] = v
+                break
+            v = stack[level] + v
+        else:
+            return v
+    raise AssertionError("unreachable")
+
+
+def test_bit_reversed_stack_adds_in_the_butterfly_order():
+    """FP64 sums of rate changes must carry the same bits in the one-warp and
+    the one-thread-per-run kernels; float64 addition here rounds as FP64 on
+    the device (round to nearest even, no fused operations)."""
+    rng = np.random.default_rng(2024)
+    for _ in range(5000):
+        p = rng.standard_normal(32) * np.exp(rng.uniform(-40.0, 40.0, 32))
+        p[rng.integers(0, 33):] = 0.0  # lanes without components add zeros
+        a, b = _butterfly([float(x) for x in p]), _bit_reversed_stack([float(x) for x in p])
+        assert np.float64(a).tobytes() == np.float64(b).tobytes()
