@@ -204,6 +204,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     w, path, blob, q = workload_blob(args.workload)
     net = api.Network(blob)
+    if args.plan:
+        net.set_plan(*[int(x) for x in args.plan.split(",")])
     n = args.runs or w.runs
     dev = torch.device("cuda", local)
     flags = torch.empty(n, dtype=torch.uint8, device=dev)
@@ -294,7 +296,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 expressions", "data": "synthetic (seeded generated network)",
         "config": bench_config(args.workload, n, world),
-        "plan": {"lanes_per_run": lanes, "comps_per_lane": cpl, "runs_per_cta": rpc},
+        "plan": {"family": r.family, "lanes_per_run": lanes, "comps_per_lane": cpl, "runs_per_cta": rpc,
+                 "forced": args.plan or None},
         "estimate": hits / runs_total,
         "race_steps_per_run": steps_total / runs_total,
         "component_steps_per_s": comp_steps / (t_total / 1000.0),
@@ -506,7 +509,7 @@ def run_batch(args):
     # the same jobs as sequential launches
     seq_ms = []
     seq_res = None
-    for _ in range(max(1, min(args.steps, 2))):
+    for _ in range(0 if args.batch_no_sequential else max(1, min(args.steps, 2))):
         t = 0.0
         seq_res = []
         for net, q, seed, runs, first in jobs:
@@ -515,9 +518,9 @@ def run_batch(args):
             seq_res.append(r)
         seq_ms.append(t)
         progress(f"sequential pass {t:.1f} ms")
-    same = all(a.hits == b.hits and a.steps == b.steps for a, b in zip(res, seq_res))
+    same = all(a.hits == b.hits and a.steps == b.steps for a, b in zip(res, seq_res)) if seq_res else None
     value = total * args.steps / (sum(batch_ms) / 1000.0)
-    seq_value = total * len(seq_ms) / (sum(seq_ms) / 1000.0)
+    seq_value = total * len(seq_ms) / (sum(seq_ms) / 1000.0) if seq_ms else None
     line = {"metric": "runs/s at 1 B200 (64 random networks in one launch)", "value": value, "unit": "runs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(batch_ms) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 state / f64 expressions",
@@ -528,8 +531,10 @@ def run_batch(args):
                        "warp_per_run_min_comps": group[0], "warp_per_run_jobs": group[1],
                        "autotuned_min_comps": tuned_min},
             "group_sweep": sweep,
-            "sequential": {"value": seq_value, "unit": "runs/s", "ms_per_step": sum(seq_ms) / len(seq_ms)},
-            "speedup_vs_sequential": value / seq_value, "results_identical_to_sequential": same,
+            "sequential": ({"value": seq_value, "unit": "runs/s", "ms_per_step": sum(seq_ms) / len(seq_ms)}
+                           if seq_ms else None),
+            "speedup_vs_sequential": value / seq_value if seq_value else None,
+            "results_identical_to_sequential": same,
             "autotune_s": t_tune, "clocks": clocks, "gpu_launches": 2 * args.steps}
     batch.close()
     for n in nets:
@@ -735,6 +740,9 @@ def main():
                     help="rare_is: exactly this many CE rounds (default: IS_CE, stopping once settled)")
     ap.add_argument("--ce-runs", type=int, default=0, help="rare_is: runs per CE round (default: IS_CE)")
     ap.add_argument("--ce-steps", type=int, default=0, help="rare_is: Adam steps per CE round (default: IS_CE)")
+    ap.add_argument("--plan", default="",
+                    help="single-network workloads: launch plan FAMILY,LANES,COMPS_PER_LANE,THREADS_PER_CTA "
+                         "(csmc_set_plan; default: the library's choice); the e2e leg keeps the default plan")
     ap.add_argument("--is-warp", action="store_true",
                     help="rare_is / is_kernel: runs under the proposal one warp per run (the thread-per-run "
                          "kernel is the default where the network qualifies)")
@@ -745,6 +753,8 @@ def main():
                     help="batch_64: networks with at least this many components run one warp per run "
                          "(0: none; -1, the default: the autotuner's choice); further comma-separated "
                          "thresholds are each timed once more and reported under group_sweep")
+    ap.add_argument("--batch-no-sequential", action="store_true",
+                    help="batch_64: skip the pass of 64 sequential launches")
     ap.add_argument("--batch-divisor", type=int, default=0,
                     help="batch_64: divide every job's run budget by this (default BATCH_BUDGET_DIVISOR)")
     ap.add_argument("--workload", default="epidemic_100", choices=sorted(WORKLOADS) + ["batch_64", "rare_is", "is_kernel", "mlp_grad"],

@@ -541,6 +541,7 @@ void csmc_net_free(csmc_net *n) {
     cudaFree(n->d_mlp);
     cudaFree(n->d_wvals);
     cudaFree(n->d_is_flags);
+    cudaFree(n->d_theta_cache);
     if (n->ev0) cudaEventDestroy(n->ev0);
     if (n->ev1) cudaEventDestroy(n->ev1);
     delete n;

@@ -52,6 +52,9 @@ struct csmc_net {
     uint32_t is_group_l = 0;
     uint32_t is_group_src[CSMC_IS_GROUPS] = {};
     int is_kernel = 0;  // 0: thread per run where the network qualifies, 3: always one warp per run
+    uint32_t *d_theta_cache = nullptr;  // thread-per-run kernel: the device-wide theta cache
+    uint32_t theta_gen = 0;             // generation of the cached parameter block (0: none yet)
+    unsigned char theta_params[CSMC_MLP_PARAM_BYTES] = {};  // the parameter block of that generation
 };
 
 namespace csmc {

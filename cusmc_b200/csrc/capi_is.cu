@@ -108,8 +108,7 @@ bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
     const bool recv = (h.recv_chan_lo | h.recv_chan_hi) != 0;
     const size_t slab = csmc::is_coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, L.block,
                                                   static_cast<uint32_t>(n->is_groups), recv);
-    L.smem = n->bytes + csmc::is_coded_mlp_smem_bytes() + (L.block / 32) * (4u * CSMC_MLP_HID * CSMC_MLP_CLASSES) +
-             slab;
+    L.smem = n->bytes + csmc::is_coded_mlp_smem_bytes() + (L.block / 32) * csmc::is_coded_warp_smem_bytes() + slab;
     if (L.smem > static_cast<size_t>(max_smem)) return false;
     if (csmc::is_coded_max_active_ctas(L.slots, L.block, L.smem, &ctas) != 0 || ctas < 1) {
         cudaGetLastError();
@@ -121,6 +120,28 @@ bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
     L.grid = static_cast<int>(grid);
     L.slab = 0;
     return true;
+}
+
+// The theta cache of the thread-per-run kernel: 2^22 entries of 32 bytes,
+// allocated on first use; a new generation (every entry free) whenever the
+// parameter block differs from the one of the current generation.
+constexpr uint32_t kThetaCacheEntries = 1u << 22;
+
+int theta_cache_for(csmc_net *n, const void *params, cudaStream_t st) {
+    const size_t bytes = static_cast<size_t>(kThetaCacheEntries) * CSMC_THETA_CACHE_WORDS * sizeof(uint32_t);
+    if (!n->d_theta_cache) {
+        CK(cudaMalloc(&n->d_theta_cache, bytes), "cudaMalloc(theta cache)");
+        CK(cudaMemsetAsync(n->d_theta_cache, 0, bytes, st), "cudaMemsetAsync(theta cache)");
+        n->theta_gen = 0;
+    }
+    if (n->theta_gen != 0 && std::memcmp(n->theta_params, params, CSMC_MLP_PARAM_BYTES) == 0) return CSMC_OK;
+    if (n->theta_gen >= 0x7fffffffu) {  // generations run out: clear the states
+        CK(cudaMemsetAsync(n->d_theta_cache, 0, bytes, st), "cudaMemsetAsync(theta cache)");
+        n->theta_gen = 0;
+    }
+    ++n->theta_gen;
+    std::memcpy(n->theta_params, params, CSMC_MLP_PARAM_BYTES);
+    return CSMC_OK;
 }
 
 csmc::IsParams base_params(const csmc_net *n, const csmc_query *q, uint64_t seed, uint64_t first_run,
@@ -237,6 +258,13 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
     ip.s.steps = steps;
     ip.logw = logw;
     ip.wvals = n->d_wvals;
+    if (coded) {
+        rc = theta_cache_for(n, params, st);
+        if (rc) return rc;
+        ip.theta_cache = n->d_theta_cache;
+        ip.cache_mask = kThetaCacheEntries - 1;
+        ip.cache_gen = n->theta_gen;
+    }
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
     rc = coded ? csmc::is_coded_launch(L.slots, ip, L.grid, L.block, L.smem, st)
                : csmc::is_launch(n->is_tc, false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);

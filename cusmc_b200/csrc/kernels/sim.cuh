@@ -221,7 +221,16 @@ struct IsParams {
     uint64_t group_map;
     uint32_t group_l;                       // location class of group i at bits 2i .. 2i + 1
     uint32_t group_src[CSMC_IS_GROUPS];     // 1/rate source of group i (SimParams::class_src format)
+    // thread-per-run kernel: device-wide cache of the class factors by
+    // feature vector (CSMC_THETA_CACHE_WORDS words per entry, cache_mask + 1
+    // entries; null: none); entries of other generations are empty
+    uint32_t *theta_cache;
+    uint32_t cache_mask;
+    uint32_t cache_gen;                     // the parameter block's generation (bit 31 clear, not 0)
 };
+// Theta cache entry: [0] state (generation, or generation | 1 << 31 while
+// being written), [1..3] the feature key, [4..7] the four class factors.
+#define CSMC_THETA_CACHE_WORDS 8
 
 // Importance sampling one thread per run (sim_is_coded.cuh), for networks
 // with race classes (at most 256 components, 32 locations per automaton):
@@ -230,8 +239,10 @@ struct IsParams {
 // then is_coded_slab_bytes of run state.
 int is_coded_launch(bool slots, const IsParams &p, int grid, int block, size_t smem, void *stream);
 int is_coded_max_active_ctas(bool slots, int block, size_t smem, int *ctas);
-// Shared memory of the proposal network in that kernel (the FP32 copies).
+// Shared memory of the proposal network in that kernel (the FP32 copies),
+// and of one warp's staging of the first hidden layer.
 size_t is_coded_mlp_smem_bytes();
+size_t is_coded_warp_smem_bytes();
 // Run state of a CTA of T threads: per thread and tilt group the step's
 // 1/rate, 1/rate' and FP64 rate change (4 words), then the class-coded
 // layout with one key chain set per tilt group.

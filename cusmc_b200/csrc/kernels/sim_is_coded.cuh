@@ -28,12 +28,13 @@
 // change, computed once per step from the group's 1/rate and factor.
 //
 // Theta.  theta depends only on the run's features (the class one-hot
-// aside); a thread keeps its last features and class factors and needs a
-// new evaluation only when they change.  The evaluation is the warp's: the
-// 32 lanes compute one feature row set together (theta_exact, the order of
-// the oracle's mlp_theta), once per distinct pending feature vector of the
-// warp, so every lane of a warp stays in the loop until the whole warp has
-// run out of runs.
+// aside) and the parameter block; a thread keeps its last features and
+// class factors and needs new ones only when the features change.  It looks
+// them up in a device-wide cache first; the misses are evaluated by the
+// warp: the 32 lanes compute one feature row set together (theta_exact, the
+// order of the oracle's mlp_theta), once per distinct pending feature
+// vector of the warp, and the result goes into the cache.  Every lane of a
+// warp stays in the loop until the whole warp has run out of runs.
 #pragma once
 #include <cstddef>
 
@@ -64,6 +65,167 @@ static __device__ __forceinline__ void stage_mlp_exact(MlpSmem *m, const MlpPara
     }
     if (threadIdx.x == 0) m->b3 = P->b3;
 }
+
+// ---- the device-wide theta cache -------------------------------------------
+// theta is a function of the feature vector and the parameter block alone,
+// so class factors computed by one warp serve every later run with the same
+// features.  An entry is written once per parameter generation: claimed by
+// CAS on its state word (generation | busy bit), filled, then published by
+// a release store of the generation; readers check the state with an
+// acquire load, then compare the key.  Entries of other generations are
+// free.  A lookup probes four consecutive entries.
+constexpr uint32_t kThetaBusy = 0x80000000u;
+constexpr uint32_t kThetaProbes = 4;
+
+static __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+static __device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+static __device__ __forceinline__ uint32_t theta_hash(uint32_t k0, uint32_t k1, uint32_t k2) {
+    uint32_t h = (k0 * 0x9e3779b1u) ^ (k1 * 0x85ebca77u) ^ (k2 * 0xc2b2ae3du);
+    h ^= h >> 15;
+    h *= 0x2c1b3c6du;
+    h ^= h >> 12;
+    return h;
+}
+
+// true: mfac holds the cached factors of the features.  *slot: an entry the
+// caller may claim for them after computing the factors (~0u: none).
+static __device__ __noinline__ bool theta_lookup(const IsParams &ip, uint32_t k0, uint32_t k1, uint32_t k2,
+                                                 float (&mfac)[CSMC_MLP_CLASSES], uint32_t &slot) {
+    slot = ~0u;
+    const uint32_t gen = ip.cache_gen;
+    uint32_t i = theta_hash(k0, k1, k2) & ip.cache_mask;
+    for (uint32_t probe = 0; probe < kThetaProbes; ++probe, i = (i + 1u) & ip.cache_mask) {
+        uint32_t *e = ip.theta_cache + static_cast<size_t>(i) * CSMC_THETA_CACHE_WORDS;
+        const uint32_t st = ld_acquire_u32(e);
+        if (st == gen) {
+            const uint4 a = *reinterpret_cast<const uint4 *>(e);
+            if (a.y == k0 && a.z == k1 && a.w == k2) {
+                const uint4 m = *reinterpret_cast<const uint4 *>(e + 4);
+                mfac[0] = __uint_as_float(m.x);
+                mfac[1] = __uint_as_float(m.y);
+                mfac[2] = __uint_as_float(m.z);
+                mfac[3] = __uint_as_float(m.w);
+                return true;
+            }
+            continue;
+        }
+        if (st == (gen | kThetaBusy)) continue;  // being written (its key unknown yet)
+        slot = i;                                // free for this generation
+        return false;
+    }
+    return false;
+}
+
+static __device__ __noinline__ void theta_insert(const IsParams &ip, uint32_t slot, uint32_t k0, uint32_t k1,
+                                                 uint32_t k2, const float (&mfac)[CSMC_MLP_CLASSES]) {
+    const uint32_t gen = ip.cache_gen;
+    uint32_t *e = ip.theta_cache + static_cast<size_t>(slot) * CSMC_THETA_CACHE_WORDS;
+    const uint32_t old = ld_acquire_u32(e);
+    if (old == gen || old == (gen | kThetaBusy)) return;  // taken meanwhile
+    if (atomicCAS(e, old, gen | kThetaBusy) != old) return;
+    e[1] = k0;
+    e[2] = k1;
+    e[3] = k2;
+    *reinterpret_cast<uint4 *>(e + 4) =
+        make_uint4(__float_as_uint(mfac[0]), __float_as_uint(mfac[1]), __float_as_uint(mfac[2]),
+                   __float_as_uint(mfac[3]));
+    st_release_u32(e, gen);
+}
+
+// theta of NV feature vectors at once (keys: BF16 bits of features 4..9
+// packed in pairs): the operations of theta_exact (sim_is.cuh) for each of
+// the 4 NV rows in the same order, with every weight read once for all
+// rows.  h1s: the warp's staging, 1 KB per vector.
+template <int NV>
+static __device__ __forceinline__ void theta_exact_n(const MlpSmem *m, float *h1s, const uint32_t (&key)[NV][3],
+                                                     float (&theta)[NV][CSMC_MLP_CLASSES]) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float x[NV][CSMC_MLP_IN];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+        for (int i = 0; i < CSMC_MLP_IN; ++i) x[v][i] = 0.0f;
+#pragma unroll
+        for (int w = 0; w < 3; ++w) {
+            x[v][4 + 2 * w] = __uint_as_float(key[v][w] << 16);
+            x[v][5 + 2 * w] = __uint_as_float(key[v][w] & 0xffff0000u);
+        }
+    }
+    float za[NV][4], zb[NV][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            za[v][r] = m->b1[lane];
+            zb[v][r] = m->b1[lane + 32];
+        }
+#pragma unroll
+    for (int i = 0; i < CSMC_MLP_IN; ++i) {
+        const float wa = m->w1t[i][lane], wb = m->w1t[i][lane + 32];
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (uint32_t r = 0; r < 4; ++r) {
+                const float xi = feat_of(x[v], r, i);
+                za[v][r] = f_fma(xi, wa, za[v][r]);
+                zb[v][r] = f_fma(xi, wb, zb[v][r]);
+            }
+    }
+    __syncwarp();  // the previous evaluation's readers of h1s are done
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        float4 *h4 = reinterpret_cast<float4 *>(h1s + v * (CSMC_MLP_HID * 4));
+        h4[lane] = make_float4(bf16_round(gelu_f(za[v][0])), bf16_round(gelu_f(za[v][1])),
+                               bf16_round(gelu_f(za[v][2])), bf16_round(gelu_f(za[v][3])));
+        h4[lane + 32] = make_float4(bf16_round(gelu_f(zb[v][0])), bf16_round(gelu_f(zb[v][1])),
+                                    bf16_round(gelu_f(zb[v][2])), bf16_round(gelu_f(zb[v][3])));
+    }
+    __syncwarp();
+    float ya[NV][4], yb[NV][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            ya[v][r] = m->b2[lane];
+            yb[v][r] = m->b2[lane + 32];
+        }
+#pragma unroll 4
+    for (int j = 0; j < CSMC_MLP_HID; ++j) {
+        const float wa = m->w2t[j][lane], wb = m->w2t[j][lane + 32];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float4 h = reinterpret_cast<const float4 *>(h1s + v * (CSMC_MLP_HID * 4))[j];
+            ya[v][0] = f_fma(h.x, wa, ya[v][0]);
+            ya[v][1] = f_fma(h.y, wa, ya[v][1]);
+            ya[v][2] = f_fma(h.z, wa, ya[v][2]);
+            ya[v][3] = f_fma(h.w, wa, ya[v][3]);
+            yb[v][0] = f_fma(h.x, wb, yb[v][0]);
+            yb[v][1] = f_fma(h.y, wb, yb[v][1]);
+            yb[v][2] = f_fma(h.z, wb, yb[v][2]);
+            yb[v][3] = f_fma(h.w, wb, yb[v][3]);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            float s = f_fma(gelu_f(yb[v][r]), m->w3[lane + 32], f_fma(gelu_f(ya[v][r]), m->w3[lane], 0.0f));
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s = f_add(s, __shfl_xor_sync(kFullWarp, s, off));
+            theta[v][r] = clip_theta(f_add(m->b3, s));
+        }
+}
+
+// Up to this many distinct feature vectors go through one warp evaluation.
+constexpr int kThetaBatch = 2;
 
 // The class-coded view with the tilt groups' location codes.
 struct IsCodedView : CodedView {
@@ -293,8 +455,8 @@ __global__ void __launch_bounds__(128, CSMC_IS_CODED_MIN_CTAS_PER_SM) is_coded_k
     const uint32_t T = blockDim.x, t = threadIdx.x, lane = t & 31u;
     const uint32_t NG = ip.n_groups;
     uint8_t *h1_base = smem + p.blob_bytes + kMlpExactBytes;
-    float *h1s = reinterpret_cast<float *>(h1_base) + (t >> 5) * (CSMC_MLP_HID * CSMC_MLP_CLASSES);
-    uint8_t *slab = h1_base + (T >> 5) * (4u * CSMC_MLP_HID * CSMC_MLP_CLASSES);
+    float *h1s = reinterpret_cast<float *>(h1_base) + (t >> 5) * (kThetaBatch * CSMC_MLP_HID * CSMC_MLP_CLASSES);
+    uint8_t *slab = h1_base + (T >> 5) * (4u * kThetaBatch * CSMC_MLP_HID * CSMC_MLP_CLASSES);
     const GroupRates gr{reinterpret_cast<uint32_t *>(slab) + t, T};
     const bool recv = (p.net.recv_lo | p.net.recv_hi) != 0;
     IsCodedView rv;
@@ -393,29 +555,14 @@ __global__ void __launch_bounds__(128, CSMC_IS_CODED_MIN_CTAS_PER_SM) is_coded_k
             need_theta = !theta_valid || fk0 != lk0 || fk1 != lk1 || fk2 != lk2;
         }
 
-        // ---- theta for the lanes whose features changed, one distinct
-        // feature vector at a time, evaluated by the whole warp
-        unsigned pend = __ballot_sync(kFullWarp, need_theta);
-        while (pend) {
-            const int j = __ffs(pend) - 1;
-            const uint32_t b0 = __shfl_sync(kFullWarp, fk0, j);
-            const uint32_t b1 = __shfl_sync(kFullWarp, fk1, j);
-            const uint32_t b2 = __shfl_sync(kFullWarp, fk2, j);
-            float xs[CSMC_MLP_IN];
+        // ---- theta for the lanes whose features changed: the cache, then
+        // one distinct feature vector at a time evaluated by the whole warp
+        uint32_t slot = ~0u;
+        if (need_theta && ip.theta_cache) {
+            float mc[CSMC_MLP_CLASSES];
+            if (theta_lookup(ip, fk0, fk1, fk2, mc, slot)) {
 #pragma unroll
-            for (int i = 0; i < CSMC_MLP_IN; ++i) xs[i] = 0.0f;
-            xs[4] = __uint_as_float(b0 << 16);
-            xs[5] = __uint_as_float(b0 & 0xffff0000u);
-            xs[6] = __uint_as_float(b1 << 16);
-            xs[7] = __uint_as_float(b1 & 0xffff0000u);
-            xs[8] = __uint_as_float(b2 << 16);
-            xs[9] = __uint_as_float(b2 & 0xffff0000u);
-            float theta[CSMC_MLP_CLASSES];
-            theta_exact(mlp, h1s, xs, theta);
-            const bool mine = need_theta && fk0 == b0 && fk1 == b1 && fk2 == b2;
-            if (mine) {
-#pragma unroll
-                for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) mfac[l] = tilt_factor(theta[l]);
+                for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) mfac[l] = mc[l];
                 lk0 = fk0;
                 lk1 = fk1;
                 lk2 = fk2;
@@ -423,7 +570,55 @@ __global__ void __launch_bounds__(128, CSMC_IS_CODED_MIN_CTAS_PER_SM) is_coded_k
                 need_theta = false;
                 rates_changed = true;
             }
-            pend &= ~__ballot_sync(kFullWarp, mine);
+        }
+        unsigned pend = __ballot_sync(kFullWarp, need_theta);
+        while (pend) {
+            // up to kThetaBatch distinct pending feature vectors: each from
+            // the lowest pending lane not served by the ones before it
+            uint32_t key[kThetaBatch][3];
+            int src[kThetaBatch];
+            int nv = 0;
+            unsigned left = pend;
+#pragma unroll
+            for (int v = 0; v < kThetaBatch; ++v) {
+                src[v] = -1;
+                if (!left) continue;  // warp-uniform
+                const int j = __ffs(left) - 1;
+                key[v][0] = __shfl_sync(kFullWarp, fk0, j);
+                key[v][1] = __shfl_sync(kFullWarp, fk1, j);
+                key[v][2] = __shfl_sync(kFullWarp, fk2, j);
+                src[v] = j;
+                ++nv;
+                left &= ~__ballot_sync(kFullWarp, need_theta && fk0 == key[v][0] && fk1 == key[v][1] &&
+                                                      fk2 == key[v][2]);
+            }
+            float theta[kThetaBatch][CSMC_MLP_CLASSES];
+            if (nv == 2) {
+                theta_exact_n<2>(mlp, h1s, key, theta);
+            } else {
+                uint32_t k1[1][3] = {{key[0][0], key[0][1], key[0][2]}};
+                float t1[1][CSMC_MLP_CLASSES];
+                theta_exact_n<1>(mlp, h1s, k1, t1);
+#pragma unroll
+                for (int l = 0; l < CSMC_MLP_CLASSES; ++l) theta[0][l] = t1[0][l];
+            }
+#pragma unroll
+            for (int v = 0; v < kThetaBatch; ++v) {
+                if (v >= nv) break;
+                const bool mine = need_theta && fk0 == key[v][0] && fk1 == key[v][1] && fk2 == key[v][2];
+                if (mine) {
+#pragma unroll
+                    for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) mfac[l] = tilt_factor(theta[v][l]);
+                    lk0 = fk0;
+                    lk1 = fk1;
+                    lk2 = fk2;
+                    theta_valid = true;
+                    need_theta = false;
+                    rates_changed = true;
+                    if (static_cast<int>(lane) == src[v] && slot != ~0u) theta_insert(ip, slot, fk0, fk1, fk2, mfac);
+                }
+            }
+            pend = __ballot_sync(kFullWarp, need_theta);
         }
         if (!have) continue;
 

@@ -93,6 +93,34 @@ def test_is_runs_match_the_oracle(name, kernel):
     assert r.sum == pytest.approx(wv.sum(), rel=1e-12, abs=1e-300)
 
 
+def test_theta_cache_keeps_runs_exact_across_launches():
+    """The thread-per-run kernel's device-wide theta cache is keyed by the
+    feature vector within one parameter block: launches with proposal A, then
+    B, then A again (a new generation: A's old entries are not reused), and
+    two launches in a row with the same block (the second reads entries the
+    first wrote), all equal the oracle's runs bit for bit."""
+    import torch
+    w = netgen.epidemic()
+    blob = _blob(w)
+    q = api.variable_query(w.var_id, 100, threshold=49, is_max=True, max_steps=100_000)
+    pa, pb = _random_proposal(4).pack(), _random_proposal(5).pack()
+    n = 1024
+    net = api.Network(blob)
+    P.set_inference(net, False)
+    try:
+        dev = torch.device("cuda")
+        for params, first in ((pa, 0), (pb, 0), (pa, 0), (pa, 5000)):
+            logw = torch.zeros(n, dtype=torch.float64, device=dev)
+            steps = torch.zeros(n, dtype=torch.int32, device=dev)
+            r = P.is_run(net, q, params, 23, n, first, logw=logw, steps=steps)
+            assert r.family == 5
+            cpu, _ = oracle.is_run(blob, q, params, 23, n, first)
+            assert np.array_equal(steps.cpu().numpy().view(np.uint32), cpu["steps"])
+            assert np.array_equal(logw.cpu().numpy().view(np.uint64), cpu["logw"].view(np.uint64))
+    finally:
+        net.close()
+
+
 def test_replay_rows_match_the_oracle():
     import torch
     w = netgen.epidemic()
