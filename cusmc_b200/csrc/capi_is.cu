@@ -101,19 +101,41 @@ bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
     if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device) != cudaSuccess)
         return false;
-    // a launch of few runs (a CE round) is bound by the steps of single
-    // runs: smaller CTAs spread its warps over more SMs
-    L.block = 128;
-    while (L.block > 32 && n_runs < 2ull * sms * L.block) L.block /= 2;
+    // below about four warps of runs per SM a launch is bound by its single
+    // runs' steps, which one warp per run takes faster (measured on the
+    // epidemic: 1e4 runs 134k runs/s one thread per run against 165k one
+    // warp per run; 2e4 runs 242k against 179k)
+    if (n->is_kernel == 0 && n_runs < 4ull * 32ull * static_cast<uint64_t>(sms)) return false;
+    // threads per CTA: 128 when the runs fill two CTAs per SM; a launch of
+    // fewer runs is bound by the steps of single runs, and smaller CTAs
+    // (64, 32) spread its warps over more SMs
     const bool recv = (h.recv_chan_lo | h.recv_chan_hi) != 0;
-    const size_t slab = csmc::is_coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, L.block,
-                                                  static_cast<uint32_t>(n->is_groups), recv);
-    L.smem = n->bytes + csmc::is_coded_mlp_smem_bytes() + (L.block / 32) * csmc::is_coded_warp_smem_bytes() + slab;
-    if (L.smem > static_cast<size_t>(max_smem)) return false;
-    if (csmc::is_coded_max_active_ctas(L.slots, L.block, L.smem, &ctas) != 0 || ctas < 1) {
-        cudaGetLastError();
-        return false;
+    auto smem_of = [&](int block) {
+        return n->bytes + csmc::is_coded_mlp_smem_bytes() + (block / 32) * csmc::is_coded_warp_smem_bytes() +
+               csmc::is_coded_slab_bytes(h.n_comps, h.n_vars, h.n_rate_prog, L.slots, block,
+                                         static_cast<uint32_t>(n->is_groups), recv);
+    };
+    auto resident = [&](int block) {  // CTAs per SM, 0 when it does not fit
+        int c = 0;
+        const size_t sm = smem_of(block);
+        if (sm > static_cast<size_t>(max_smem)) return 0;
+        if (csmc::is_coded_max_active_ctas(L.slots, block, sm, &c) != 0) {
+            cudaGetLastError();
+            return 0;
+        }
+        return c;
+    };
+    L.block = 0;
+    if (n_runs >= 2ull * sms * 128) {
+        ctas = resident(128);
+        if (ctas >= 1) L.block = 128;
     }
+    if (L.block == 0) {
+        L.block = n_runs >= 2ull * sms * 64 ? 64 : 32;
+        ctas = resident(L.block);
+        if (ctas < 1) return false;
+    }
+    L.smem = smem_of(L.block);
     uint64_t grid = static_cast<uint64_t>(sms) * ctas;
     const uint64_t needed = (n_runs + L.block - 1) / L.block;
     if (grid > needed) grid = needed;
@@ -190,7 +212,8 @@ int csmc_is_set_inference(csmc_net *n, int32_t tensor_cores) {
 
 int csmc_is_set_kernel(csmc_net *n, int32_t family) {
     if (!n) return fail(CSMC_ERR_ARG, "null argument");
-    if (family != 0 && family != 3) return fail(CSMC_ERR_ARG, "importance-sampling kernel family must be 0 or 3");
+    if (family != 0 && family != 3 && family != 5)
+        return fail(CSMC_ERR_ARG, "importance-sampling kernel family must be 0, 3 or 5");
     n->is_kernel = family;
     return CSMC_OK;
 }

@@ -41,6 +41,12 @@
 #include "sim_coded.cuh"
 #include "sim_is.cuh"
 
+// Up to 128 threads per CTA.  192-thread CTAs (two per SM, twelve warps)
+// measured slower on the epidemic (561k against 577k-591k runs/s at 1e5
+// runs).
+#ifndef CSMC_IS_CODED_MAX_THREADS
+#define CSMC_IS_CODED_MAX_THREADS 128
+#endif
 #ifndef CSMC_IS_CODED_MIN_CTAS_PER_SM
 #define CSMC_IS_CODED_MIN_CTAS_PER_SM 3
 #endif
@@ -224,8 +230,9 @@ static __device__ __forceinline__ void theta_exact_n(const MlpSmem *m, float *h1
         }
 }
 
-// Up to this many distinct feature vectors go through one warp evaluation.
-constexpr int kThetaBatch = 2;
+// Distinct feature vectors per warp evaluation: evaluating two at once
+// (every weight read once for eight rows) measured no faster than one.
+constexpr int kThetaBatch = 1;
 
 // The class-coded view with the tilt groups' location codes.
 struct IsCodedView : CodedView {
@@ -445,7 +452,8 @@ static __device__ __forceinline__ bool is_race_coded(const Net &n, uint32_t C, u
 }
 
 template <bool SLOTS>
-__global__ void __launch_bounds__(128, CSMC_IS_CODED_MIN_CTAS_PER_SM) is_coded_kernel(const __grid_constant__ IsParams ip) {
+__global__ void __launch_bounds__(CSMC_IS_CODED_MAX_THREADS, CSMC_IS_CODED_MIN_CTAS_PER_SM)
+    is_coded_kernel(const __grid_constant__ IsParams ip) {
     const SimParams &p = ip.s;
     extern __shared__ __align__(16) uint8_t smem[];
     stage_network(smem, p.blob, p.blob_bytes);
@@ -573,52 +581,24 @@ __global__ void __launch_bounds__(128, CSMC_IS_CODED_MIN_CTAS_PER_SM) is_coded_k
         }
         unsigned pend = __ballot_sync(kFullWarp, need_theta);
         while (pend) {
-            // up to kThetaBatch distinct pending feature vectors: each from
-            // the lowest pending lane not served by the ones before it
-            uint32_t key[kThetaBatch][3];
-            int src[kThetaBatch];
-            int nv = 0;
-            unsigned left = pend;
+            const int j = __ffs(pend) - 1;
+            uint32_t key[1][3] = {{__shfl_sync(kFullWarp, fk0, j), __shfl_sync(kFullWarp, fk1, j),
+                                   __shfl_sync(kFullWarp, fk2, j)}};
+            float theta[1][CSMC_MLP_CLASSES];
+            theta_exact_n<1>(mlp, h1s, key, theta);
+            const bool mine = need_theta && fk0 == key[0][0] && fk1 == key[0][1] && fk2 == key[0][2];
+            if (mine) {
 #pragma unroll
-            for (int v = 0; v < kThetaBatch; ++v) {
-                src[v] = -1;
-                if (!left) continue;  // warp-uniform
-                const int j = __ffs(left) - 1;
-                key[v][0] = __shfl_sync(kFullWarp, fk0, j);
-                key[v][1] = __shfl_sync(kFullWarp, fk1, j);
-                key[v][2] = __shfl_sync(kFullWarp, fk2, j);
-                src[v] = j;
-                ++nv;
-                left &= ~__ballot_sync(kFullWarp, need_theta && fk0 == key[v][0] && fk1 == key[v][1] &&
-                                                      fk2 == key[v][2]);
+                for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) mfac[l] = tilt_factor(theta[0][l]);
+                lk0 = fk0;
+                lk1 = fk1;
+                lk2 = fk2;
+                theta_valid = true;
+                need_theta = false;
+                rates_changed = true;
+                if (static_cast<int>(lane) == j && slot != ~0u) theta_insert(ip, slot, fk0, fk1, fk2, mfac);
             }
-            float theta[kThetaBatch][CSMC_MLP_CLASSES];
-            if (nv == 2) {
-                theta_exact_n<2>(mlp, h1s, key, theta);
-            } else {
-                uint32_t k1[1][3] = {{key[0][0], key[0][1], key[0][2]}};
-                float t1[1][CSMC_MLP_CLASSES];
-                theta_exact_n<1>(mlp, h1s, k1, t1);
-#pragma unroll
-                for (int l = 0; l < CSMC_MLP_CLASSES; ++l) theta[0][l] = t1[0][l];
-            }
-#pragma unroll
-            for (int v = 0; v < kThetaBatch; ++v) {
-                if (v >= nv) break;
-                const bool mine = need_theta && fk0 == key[v][0] && fk1 == key[v][1] && fk2 == key[v][2];
-                if (mine) {
-#pragma unroll
-                    for (uint32_t l = 0; l < CSMC_MLP_CLASSES; ++l) mfac[l] = tilt_factor(theta[v][l]);
-                    lk0 = fk0;
-                    lk1 = fk1;
-                    lk2 = fk2;
-                    theta_valid = true;
-                    need_theta = false;
-                    rates_changed = true;
-                    if (static_cast<int>(lane) == src[v] && slot != ~0u) theta_insert(ip, slot, fk0, fk1, fk2, mfac);
-                }
-            }
-            pend = __ballot_sync(kFullWarp, need_theta);
+            pend &= ~__ballot_sync(kFullWarp, mine);
         }
         if (!have) continue;
 

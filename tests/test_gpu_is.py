@@ -56,12 +56,12 @@ CASES = {
 }
 
 
-# networks with race classes: csmc_is_run simulates them one thread per run
-# (family 5) unless told to use one warp per run (family 3)
+# networks with race classes: csmc_is_set_kernel(5) simulates them one
+# thread per run (family 5) at any launch size; 3 forces one warp per run
 THREAD_CASES = {"epidemic", "epidemic_160", "mutex"}
 
 
-@pytest.mark.parametrize("kernel", [0, 3])
+@pytest.mark.parametrize("kernel", [5, 3])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_is_runs_match_the_oracle(name, kernel):
     import torch
@@ -83,7 +83,7 @@ def test_is_runs_match_the_oracle(name, kernel):
         r = P.is_run(net, q, params, 17, n, 40, flags=flags, logw=logw, values=values, steps=steps)
     finally:
         net.close()
-    assert r.family == (5 if kernel == 0 and name in THREAD_CASES else 3)
+    assert r.family == (5 if kernel == 5 and name in THREAD_CASES else 3)
     cpu, _ = oracle.is_run(blob, q, params, 17, n, 40)
     assert np.array_equal(flags.cpu().numpy(), cpu["flags"])
     assert np.array_equal(steps.cpu().numpy().view(np.uint32), cpu["steps"])
@@ -107,6 +107,7 @@ def test_theta_cache_keeps_runs_exact_across_launches():
     n = 1024
     net = api.Network(blob)
     P.set_inference(net, False)
+    P.set_kernel(net, 5)
     try:
         dev = torch.device("cuda")
         for params, first in ((pa, 0), (pb, 0), (pa, 0), (pa, 5000)):
