@@ -583,8 +583,8 @@ def run_rare_is(args):
         if (p > 0 and half <= 0.1 * p) or n >= 10_000_000:
             break
     is_s = time.perf_counter() - t1
-    # optional fixed-size evaluation of the trained proposal (the survey's
-    # protocol: 1e7 weighted runs), outside the timed figure
+    # optional fixed-size evaluation of the trained proposal (for example
+    # 1e7 weighted runs), outside the timed figure
     evaluation = None
     if args.is_eval_runs:
         t_eval = time.perf_counter()
