@@ -121,6 +121,39 @@ def test_large_networks_one_warp_per_run_match_single_runs():
             j[0].close()
 
 
+@pytest.mark.parametrize("specs,k_expect", [
+    # largest network 100 components: 4 per lane
+    ([("epidemic", 300), ("mutex32", 400), ("random0", 600)], 4),
+    # largest 230 components: 8 per lane
+    ([("big7", 40), ("mutex8", 500)], 8),
+])
+def test_every_lane_width_of_warp_per_run_jobs(specs, k_expect):
+    """Every job one warp per run (threshold 2), with the largest network
+    choosing 4 or 8 components per lane, against csmc_run_verify."""
+    make = {"epidemic": netgen.epidemic, "mutex32": lambda: netgen.mutex(32), "mutex8": lambda: netgen.mutex(8),
+            "random0": lambda: netgen.random_network(0),
+            "big7": lambda: netgen.batch_networks(count=8, base_seed=1000)[7]}
+    jobs = []
+    for i, (name, runs) in enumerate(specs):
+        w = make[name]()
+        net = api.Network(_blob(w))
+        q = api.variable_query(w.var_id, w.horizon, threshold=w.threshold, is_max=True, max_steps=100_000)
+        jobs.append((net, q, 9300 + i, runs, 3 * i))
+    singles = [_single(*j) for j in jobs]
+    batch = api.Batch(jobs, verify=True)
+    try:
+        batch.set_group_comps(2)
+        assert batch.group_comps() == (2, len(jobs))
+        res = batch.run(use_graph=False)
+        for i in range(len(jobs)):
+            _assert_job_equal(res[i], batch.outputs(i), *singles[i])
+            assert res[i].lanes_per_run == 32 and res[i].comps_per_lane == k_expect
+    finally:
+        batch.close()
+        for j in jobs:
+            j[0].close()
+
+
 @pytest.mark.parametrize("group_comps", [0, 2])
 def test_batch_job_against_the_oracle(group_comps):
     import oracle
