@@ -46,7 +46,31 @@ def _random_proposal(seed, out_scale=0.3):
     return p
 
 
+def _tilt_mix(n_comps=24):
+    """Components of four exponential locations in a cycle whose rates come
+    from four shared literals rotated by component, so every rate appears in
+    every location class: 16 (race class, location class) pairs, more than
+    the six tilt groups (the rest take the descriptor path).  Leaving L3
+    broadcasts `go`, which moves receivers in L1 to L2 (L1 has two edges, so
+    slot masks are kept); counters v0..v3 feed the proposal's features."""
+    rates = ["0.3", "0.7", "1.1", "1.9"]
+    d = netgen._Doc("int v0 = 0;\nint v1 = 0;\nint v2 = 0;\nint v3 = 0;\nbroadcast chan go;")
+    for c in range(n_comps):
+        ids = [d.new_id() for _ in range(4)]
+        locs = [(ids[i], f"L{i}", [("exponentialrate", rates[(i + c) % 4])]) for i in range(4)]
+        trans = [
+            (ids[0], ids[1], [("assignment", "v1 = v1 + 1")]),
+            (ids[1], ids[2], [("assignment", "v2 = v2 + 1")]),
+            (ids[1], ids[2], [("synchronisation", "go?")]),
+            (ids[2], ids[3], [("assignment", "v3 = v3 + 1")]),
+            (ids[3], ids[0], [("synchronisation", "go!"), ("assignment", "v0 = v0 + 1")]),
+        ]
+        d.template(f"M{c}", "", locs, ids[0], trans)
+    return netgen.Workload("tilt_mix", d.finish(), var_id=0, threshold=46, horizon=15, runs=1000, n_vars=4)
+
+
 CASES = {
+    "tilt_mix": lambda: (_tilt_mix(), None, None),
     "epidemic": lambda: (netgen.epidemic(), 100, 49),
     # 160 components: lanes 0..7 of the warp draw two Philox blocks each, so
     # their partial sums span two blocks (the warp order of csmc_mlp.h)
@@ -58,7 +82,7 @@ CASES = {
 
 # networks with race classes: csmc_is_set_kernel(5) simulates them one
 # thread per run (family 5) at any launch size; 3 forces one warp per run
-THREAD_CASES = {"epidemic", "epidemic_160", "mutex"}
+THREAD_CASES = {"epidemic", "epidemic_160", "mutex", "tilt_mix"}
 
 
 @pytest.mark.parametrize("kernel", [5, 3])
