@@ -188,7 +188,7 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
     const uint64_t n = cfg.runs_per_round;
     std::vector<float> x(init, init + kFloats);
     Adam opt(cfg.lr);
-    DevBuf d_flags, d_logw, d_values, d_steps, d_rows, d_elite, d_w, d_off;
+    DevBuf d_flags, d_logw, d_values, d_steps, d_rows, d_merged, d_elite, d_w, d_off;
     cudaError_t e = d_flags.ensure(n);
     if (e == cudaSuccess) e = d_logw.ensure(n * sizeof(double));
     if (e == cudaSuccess) e = d_values.ensure(n * sizeof(double));
@@ -215,6 +215,7 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
                                    cfg.rho, cfg.max_rows);
         const size_t m = s.elite.size();
         e = d_rows.ensure(std::max<uint64_t>(1, s.n_rows) * kRowBytes);
+        if (e == cudaSuccess) e = d_merged.ensure(std::max<uint64_t>(1, s.n_rows) * kRowBytes);
         if (e == cudaSuccess) e = d_elite.ensure(m * sizeof(uint64_t));
         if (e == cudaSuccess) e = d_w.ensure(m * sizeof(float));
         if (e == cudaSuccess) e = d_off.ensure(m * sizeof(uint64_t));
@@ -228,12 +229,16 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
         rc = csmc_is_trace(net, q, &P, seed, first, d_elite.as<uint64_t>(), d_w.as<float>(), d_off.as<uint64_t>(), m,
                            d_rows.p, d_rows.bytes / kRowBytes, nullptr);
         if (rc) return rc;
+        // rows of equal features on consecutive steps summed (J unchanged)
+        uint64_t m_rows = 0;
+        rc = csmc_mlp_rows_merge(d_rows.p, d_off.as<uint64_t>(), m, s.n_rows, d_merged.p, &m_rows, nullptr);
+        if (rc) return rc;
         const double trace_s = seconds_since(t1);
         const auto t2 = std::chrono::steady_clock::now();
         double J0 = 0.0, J = 0.0;
         for (int32_t st = 0; st < cfg.adam_steps; ++st) {
             pack(x.data(), P);
-            rc = csmc_mlp_grad(&P, d_rows.p, s.n_rows, g.data(), &J, nullptr);
+            rc = csmc_mlp_grad(&P, d_merged.p, m_rows, g.data(), &J, nullptr);
             if (rc) return rc;
             if (st == 0) J0 = J;
             opt.ascend(x.data(), g.data());

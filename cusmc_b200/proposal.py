@@ -174,6 +174,15 @@ def mlp_forward(params: bytes, rows, n_rows: int, theta, stream=None) -> None:
     check(lib().csmc_mlp_forward(params, _ptr(rows), n_rows, _ptr(theta), stream))
 
 
+def merge_rows(rows, row_offset, n_list: int, n_rows: int, out, stream=None) -> int:
+    """csmc_mlp_rows_merge: rows, row_offset (the replay's per-run first
+    rows) and out are torch CUDA tensors; returns the merged row count."""
+    n = ctypes.c_uint64()
+    check(lib().csmc_mlp_rows_merge(_ptr(rows), _ptr(row_offset), n_list, n_rows, _ptr(out), ctypes.byref(n),
+                                    stream))
+    return n.value
+
+
 def mlp_grad(params: bytes, rows, n_rows: int, stream=None):
     g = np.zeros(GRAD_FLOATS, np.float32)
     J = ctypes.c_double()
@@ -318,25 +327,29 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
         t_off = torch.from_numpy(sel.row_offset.view(np.int64)).to(dev)
         t1 = time.perf_counter()
         is_trace(net, query, params, seed, t_runs, t_w, t_off, rows, first)
+        # rows of equal features on consecutive steps summed (J unchanged)
+        merged = torch.empty_like(rows)
+        m_rows = merge_rows(rows, t_off, len(elite), n_rows, merged)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         J0 = None
         for _ in range(adam_steps):
-            g, J = mlp_grad(prop.pack(), rows, n_rows)
+            g, J = mlp_grad(prop.pack(), merged, m_rows)
             if J0 is None:
                 J0 = J
             x = opt.ascend(x, g)
             prop = Proposal.from_vector(x)
         t3 = time.perf_counter()
         hit_est = float(res.estimate)
-        entry = {"round": k, "level": sel.level, "elite": int(len(elite)), "rows": n_rows, "J_start": J0, "J_end": J,
+        entry = {"round": k, "level": sel.level, "elite": int(len(elite)), "rows": n_rows, "merged_rows": m_rows,
+                 "J_start": J0, "J_end": J,
                  "estimate": hit_est, "hits": int(res.hits), "mean_steps": res.steps / max(res.runs, 1),
                  "capped": int(res.capped), "kernel_ms": res.kernel_ms, "run_s": t1 - t0, "trace_s": t2 - t1,
                  "adam_s": t3 - t2, "seconds": t3 - t0}
         log.rounds.append(entry)
         if verbose:
             print(entry, flush=True)
-        del rows
+        del rows, merged
         at_goal = at_goal + 1 if sel.at_goal else 0
         if settle and at_goal >= settle:
             break

@@ -326,6 +326,17 @@ int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, floa
 int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
                   void *stream);
 
+/* Merges replayed training rows (device buffers): rows of one listed run and
+ * one location class (rows row_offset[i] + l, + 4, ..., up to the next
+ * run's first row or n_rows) whose features are equal on consecutive steps
+ * are summed into one row (a and b added in FP64 in step order, rounded to
+ * FP32), and rows whose a and b are both zero are dropped.  J and its
+ * gradient are unchanged in exact arithmetic (J is linear in a and b for a
+ * fixed feature row).  out (device, room for n_rows rows) receives the
+ * merged rows, ordered by run, class and first step; *n_out their count. */
+int csmc_mlp_rows_merge(const void *rows, const uint64_t *row_offset, uint64_t n_list, uint64_t n_rows, void *out,
+                        uint64_t *n_out, void *stream);
+
 /* ---- Cross-entropy training of the proposal ---------------------------
  * No counterpart in the reference.  The reference's entry point for a run
  * of the statistical model checker is smc() (smc.cuh:14, smc.cu:283-491);

@@ -199,6 +199,62 @@ def test_replay_rows_match_the_oracle():
     assert got.tobytes() == cpu_rows.tobytes()
 
 
+def _merge_rows_reference(rows, offs):
+    """csmc_mlp_rows_merge restated: per run and class, consecutive rows of
+    equal features summed (FP64, step order, rounded to FP32); all-zero
+    groups dropped; run-major, then class, then first step."""
+    out = []
+    n = len(rows)
+    for i, b in enumerate(offs):
+        e = offs[i + 1] if i + 1 < len(offs) else n
+        for l in range(4):
+            key, head, sa, sb = None, None, 0.0, 0.0
+            for r in range(b + l, e, 4):
+                x = rows["x"][r].tobytes()
+                if x != key:
+                    if key is not None and (sa != 0.0 or sb != 0.0):
+                        out.append((rows["x"][head], np.float32(sa), np.float32(sb)))
+                    key, head, sa, sb = x, r, 0.0, 0.0
+                sa += float(rows["a"][r])
+                sb += float(rows["b"][r])
+            if key is not None and (sa != 0.0 or sb != 0.0):
+                out.append((rows["x"][head], np.float32(sa), np.float32(sb)))
+    res = np.zeros(len(out), dtype=rows.dtype)
+    for k, (x, sa, sb) in enumerate(out):
+        res["x"][k] = x
+        res["a"][k] = sa
+        res["b"][k] = sb
+    return res
+
+
+def test_row_merge_keeps_the_objective_and_gradient():
+    """Replayed rows merged on the GPU equal the restated merge byte for byte
+    and give the same J and gradient up to rounding."""
+    import torch
+    w = netgen.epidemic()
+    blob = _blob(w)
+    q = api.variable_query(w.var_id, 100, threshold=49, is_max=True)
+    params = _random_proposal(8).pack()
+    runs = np.array([0, 3, 5, 11, 40, 77], dtype=np.uint64)
+    weights = np.array([0.1, 0.2, 0.3, 0.15, 0.25, 0.05], dtype=np.float32)
+    cpu_rows = oracle.is_trace(blob, q, params, 21, runs, weights, first_run=7)
+    cpu_out, _ = oracle.is_run(blob, q, params, 21, 78, 7)
+    st = cpu_out["steps"][runs.astype(np.int64)].astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(4 * st)[:-1]]).astype(np.uint64)
+    dev = torch.device("cuda")
+    rows = torch.from_numpy(cpu_rows.view(np.uint8).copy()).to(dev)
+    merged = torch.zeros_like(rows)
+    n = P.merge_rows(rows, torch.from_numpy(offs.view(np.int64)).to(dev), len(runs), len(cpu_rows), merged)
+    ref = _merge_rows_reference(cpu_rows, [int(o) for o in offs])
+    assert n == len(ref) and n < len(cpu_rows) // 2
+    got = merged.cpu().numpy()[: n * P.ROW_BYTES].view(oracle.ROW_DTYPE)
+    assert got.tobytes() == ref.tobytes()
+    g0, j0 = P.mlp_grad(params, rows, len(cpu_rows))
+    g1, j1 = P.mlp_grad(params, merged, n)
+    assert j1 == pytest.approx(j0, rel=1e-5)
+    assert np.linalg.norm(g1 - g0) <= 1e-3 * np.linalg.norm(g0)
+
+
 def test_tensor_core_inference_follows_the_exact_paths():
     import torch
     w = netgen.epidemic()
