@@ -100,22 +100,23 @@ static __device__ __forceinline__ float desc_delay(const Net &n, const CodedView
 }
 
 // One component's part in the race: a class member updates its class's
-// chain-k pair, any other component (ALLCLS false) races with its own delay.
-// br: the component's bit-reversed index (bitrev_bits(cc, bits)).
+// chain-k largest key, any other component (ALLCLS false) races with its own
+// delay.  cb: 255 minus the component's bit-reversed index (bitrev_bits(cc,
+// bits)), the low byte of its class key: (x | 0xff) - br = (x & ~0xff) | cb.
 template <bool ALLCLS, uint32_t k>
 static __device__ __forceinline__ void race_member(const Net &n, uint32_t bits, const CodedView &rv, uint32_t wd,
-                                                   uint32_t cc, uint32_t x, uint32_t br, unsigned long long &best,
+                                                   uint32_t cc, uint32_t x, uint32_t cb, unsigned long long &best,
                                                    float &bestd) {
     const uint32_t b = (wd >> (8u * k)) & 0xffu;
     const uint32_t code = b >> 5;
     const uint32_t T = rv.T;
     if (ALLCLS || code < CSMC_RACE_CLASSES) {
-        const uint32_t key = (x | 0xffu) - br;
+        const uint32_t key = (x & 0xffffff00u) | cb;
         uint32_t *pp = rv.keys + (code * 4u + k) * T;
         *pp = max(*pp, key);
     } else if (code == kCodeGeneral) {
         const float d = desc_delay(n, rv, n.comp[cc].loc_begin + (b & 31u), x);
-        const unsigned long long key = (static_cast<unsigned long long>(delay_key(d)) << 32) | br;
+        const unsigned long long key = (static_cast<unsigned long long>(delay_key(d)) << 32) | (255u - cb);
         if (key < best) {
             best = key;
             bestd = d;
@@ -146,18 +147,20 @@ static __device__ __forceinline__ bool race_coded(const Net &n, uint32_t C, uint
         const u32x4 blk = philox_block(K, ps, q);
         const uint32_t wd = rv.lw[q * T], cc = 4u * q;
         const uint32_t rq = hi_shift ? (__brev(q) >> (32u - hi_shift)) : 0u;
-        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, rq, best, bestd);
-        race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, rq + (2u << hi_shift), best, bestd);
-        race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, rq + (1u << hi_shift), best, bestd);
-        race_member<ALLCLS, 3>(n, bits, rv, wd, cc + 3u, blk.w, rq + (3u << hi_shift), best, bestd);
+        const uint32_t cb = 255u - rq;
+        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, cb, best, bestd);
+        race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, cb - (2u << hi_shift), best, bestd);
+        race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, cb - (1u << hi_shift), best, bestd);
+        race_member<ALLCLS, 3>(n, bits, rv, wd, cc + 3u, blk.w, cb - (3u << hi_shift), best, bestd);
     }
     if (C & 3u) {  // the last, partly filled word
         const u32x4 blk = philox_block(K, ps, Qf);
         const uint32_t wd = rv.lw[Qf * T], cc = 4u * Qf, rem = C & 3u;
         const uint32_t rq = hi_shift ? (__brev(Qf) >> (32u - hi_shift)) : 0u;
-        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, rq, best, bestd);
-        if (rem > 1u) race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, rq + (2u << hi_shift), best, bestd);
-        if (rem > 2u) race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, rq + (1u << hi_shift), best, bestd);
+        const uint32_t cb = 255u - rq;
+        race_member<ALLCLS, 0>(n, bits, rv, wd, cc, blk.x, cb, best, bestd);
+        if (rem > 1u) race_member<ALLCLS, 1>(n, bits, rv, wd, cc + 1u, blk.y, cb - (2u << hi_shift), best, bestd);
+        if (rem > 2u) race_member<ALLCLS, 2>(n, bits, rv, wd, cc + 2u, blk.z, cb - (1u << hi_shift), best, bestd);
     }
     // each class races with its largest key
     uint32_t inf_classes = 0, ties = 0;
