@@ -557,6 +557,8 @@ def run_rare_is(args):
         P.set_inference(net, True)
     if args.is_warp:
         P.set_kernel(net, 3)
+    elif args.is_thread:
+        P.set_kernel(net, 5)
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
     ce = dict(IS_CE)
@@ -648,6 +650,8 @@ def run_is_kernel(args):
         P.set_inference(net, True)
     if args.is_warp:
         P.set_kernel(net, 3)
+    elif args.is_thread:
+        P.set_kernel(net, 5)
     T, thr = IS_RARE
     q = api.variable_query(w.var_id, T, threshold=thr, is_max=True)
     prop, log = P.train(net, q, seed=1, **IS_CE)
@@ -754,6 +758,9 @@ def main():
     ap.add_argument("--is-warp", action="store_true",
                     help="rare_is / is_kernel: runs under the proposal one warp per run (the thread-per-run "
                          "kernel is the default where the network qualifies)")
+    ap.add_argument("--is-thread", action="store_true",
+                    help="rare_is / is_kernel: runs under the proposal one thread per run at every launch size "
+                         "(the default takes one warp per run below 48 runs per SM on the epidemic)")
     ap.add_argument("--is-tc", action="store_true",
                     help="rare_is / is_kernel: theta by warp-level tensor-core MMAs instead of the CUDA-core "
                          "evaluation in the oracle's order")

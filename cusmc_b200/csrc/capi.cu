@@ -501,6 +501,10 @@ int csmc_net_upload(const void *blob, size_t bytes, csmc_net **out) {
                     map |= static_cast<uint64_t>(id[g][l] < 0 ? 7 : id[g][l]) << (3 * (4 * g + l));
             n->is_group_map = map;
             n->is_groups = groups;
+            bool spill = false;  // a classed location's pair beyond the groups
+            for (uint32_t g = 0; g < CSMC_RACE_CLASSES; ++g)
+                for (uint32_t l = 0; l < 4; ++l) spill = spill || id[g][l] == 7;
+            n->is_all_grouped = n->all_classed && !spill && h->n_comps % 4 == 0;
         }
     }
     // default plan: the class-coded thread-per-run kernel when the network

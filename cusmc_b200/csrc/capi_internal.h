@@ -48,6 +48,7 @@ struct csmc_net {
     // importance sampling one thread per run (sim_is_coded.cuh): the tilt
     // groups of the network (is_groups < 0: the network does not qualify)
     int is_groups = -1;
+    bool is_all_grouped = false;  // every location in a tilt group, components a multiple of 4
     uint64_t is_group_map = 0;
     uint32_t is_group_l = 0;
     uint32_t is_group_src[CSMC_IS_GROUPS] = {};

@@ -101,11 +101,16 @@ bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
     if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, n->device) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device) != cudaSuccess)
         return false;
-    // below about four warps of runs per SM a launch is bound by its single
-    // runs' steps, which one warp per run takes faster (measured on the
-    // epidemic: 1e4 runs 134k runs/s one thread per run against 165k one
-    // warp per run; 2e4 runs 242k against 179k)
-    if (n->is_kernel == 0 && n_runs < 4ull * 32ull * static_cast<uint64_t>(sms)) return false;
+    // a small launch is bound by its single runs' steps, which one warp per
+    // run takes faster.  The crossover, measured on the epidemic under a
+    // trained proposal: with every location in a tilt group (no descriptor
+    // path), one thread per run takes ~45 ms per launch up to a full GPU
+    // and one warp per run ~6.1 us per run (5e3 runs: 44.5 against 33.4 ms;
+    // 1e4 runs: 45.3 against 60.8 ms), so one thread per run from 48 runs
+    // per SM; with the descriptor path, from 128 runs per SM (1e4 runs:
+    // 134k runs/s against 165k; 2e4 runs: 242k against 179k)
+    const uint64_t min_runs = (n->is_all_grouped ? 48ull : 128ull) * static_cast<uint64_t>(sms);
+    if (n->is_kernel == 0 && n_runs < min_runs) return false;
     // threads per CTA: 128 when the runs fill two CTAs per SM; a launch of
     // fewer runs is bound by the steps of single runs, and smaller CTAs
     // (64, 32) spread its warps over more SMs
@@ -119,7 +124,7 @@ bool plan_is_coded(const csmc_net *n, uint64_t n_runs, Launch &L) {
         int c = 0;
         const size_t sm = smem_of(block);
         if (sm > static_cast<size_t>(max_smem)) return 0;
-        if (csmc::is_coded_max_active_ctas(L.slots, block, sm, &c) != 0) {
+        if (csmc::is_coded_max_active_ctas(L.slots, n->is_all_grouped, block, sm, &c) != 0) {
             cudaGetLastError();
             return 0;
         }
@@ -289,7 +294,7 @@ int csmc_is_run(csmc_net *n, const csmc_query *q, const void *params, uint64_t s
         ip.cache_gen = n->theta_gen;
     }
     CK(cudaEventRecord(n->ev0, st), "cudaEventRecord");
-    rc = coded ? csmc::is_coded_launch(L.slots, ip, L.grid, L.block, L.smem, st)
+    rc = coded ? csmc::is_coded_launch(L.slots, n->is_all_grouped, ip, L.grid, L.block, L.smem, st)
                : csmc::is_launch(n->is_tc, false, L.slots, L.loc8, ip, L.grid, L.block, L.smem, st);
     if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "importance-sampling kernel launch");
     CK(cudaEventRecord(n->ev1, st), "cudaEventRecord");

@@ -237,8 +237,10 @@ struct IsParams {
 // the CUDA-core evaluation of theta, no trace mode.  Shared memory: the
 // network, the proposal network's FP32 copies, each warp's first-hidden-layer staging,
 // then is_coded_slab_bytes of run state.
-int is_coded_launch(bool slots, const IsParams &p, int grid, int block, size_t smem, void *stream);
-int is_coded_max_active_ctas(bool slots, int block, size_t smem, int *ctas);
+// all_grouped: every location belongs to a tilt group and the component
+// count is a multiple of four (no descriptor path, no padding in the race).
+int is_coded_launch(bool slots, bool all_grouped, const IsParams &p, int grid, int block, size_t smem, void *stream);
+int is_coded_max_active_ctas(bool slots, bool all_grouped, int block, size_t smem, int *ctas);
 // Shared memory of the proposal network in that kernel (the FP32 copies),
 // and of one warp's staging of the first hidden layer.
 size_t is_coded_mlp_smem_bytes();

@@ -304,17 +304,20 @@ static __device__ __forceinline__ void is_take(IsBest &b, unsigned long long key
     }
 }
 
-// One component's part in the race and in its lane's partial sum.
-template <uint32_t k>
+// One component's part in the race and in its lane's partial sum.  cb:
+// 255 minus the component's bit-reversed index, the low byte of its group
+// key.  ALLG: every component is a group member (no descriptor path, no
+// padding).
+template <bool ALLG, uint32_t k>
 static __device__ __forceinline__ void is_member(const Net &n, const IsCodedView &rv, const GroupRates &gr,
                                                  uint32_t NG, uint32_t tilt_mask, const float (&mfac)[CSMC_MLP_CLASSES],
-                                                 uint32_t wd, uint32_t cc, uint32_t x, uint32_t br, IsBest &best,
+                                                 uint32_t wd, uint32_t cc, uint32_t x, uint32_t cb, IsBest &best,
                                                  double &part) {
     const uint32_t b = (wd >> (8u * k)) & 0xffu;
     const uint32_t code = b >> 5;
     const uint32_t T = rv.T;
-    if (code < NG) {
-        const uint32_t key = (x | 0xffu) - br;
+    if (ALLG || code < NG) {
+        const uint32_t key = (x & 0xffffff00u) | cb;
         uint32_t *pp = rv.keys + (code * 4u + k) * T;
         *pp = max(*pp, key);
         if ((tilt_mask >> code) & 1u) part = d_add(part, gr.diff(code));
@@ -324,7 +327,7 @@ static __device__ __forceinline__ void is_member(const Net &n, const IsCodedView
         float inv, invp;
         const float d = is_desc_delay(n, rv.vars, rv.rates, n.comp[cc].loc_begin + local, x, mfac_of(mfac, local & 3u),
                                       tl, inv, invp);
-        is_take(best, (static_cast<unsigned long long>(delay_key(d)) << 32) | br, d, inv, invp, tl);
+        is_take(best, (static_cast<unsigned long long>(delay_key(d)) << 32) | (255u - cb), d, inv, invp, tl);
         if (tl) part = d_add(part, rate_change(inv, invp));
     }
 }
@@ -384,6 +387,7 @@ static __device__ __forceinline__ void tree_push(uint32_t i, double v, double (&
 // The step's race and sum of rate changes.  Returns false when the groups'
 // keys do not decide the race (the caller runs is_race_exact); `sum` is
 // valid either way.
+template <bool ALLG>
 static __device__ __forceinline__ bool is_race_coded(const Net &n, uint32_t C, uint32_t bits, uint32_t NG,
                                                      uint32_t tilt_mask, const IsCodedView &rv, const GroupRates &gr,
                                                      const float (&mfac)[CSMC_MLP_CLASSES], const PhiloxKeys &K,
@@ -405,10 +409,11 @@ static __device__ __forceinline__ bool is_race_coded(const Net &n, uint32_t C, u
             const u32x4 blk = philox_block(K, ps, q);
             const uint32_t wd = rv.lw[q * T], cc = 4u * q;
             const uint32_t rq = hi_shift ? (__brev(q) >> (32u - hi_shift)) : 0u;
-            is_member<0>(n, rv, gr, NG, tilt_mask, mfac, wd, cc, blk.x, rq, best, part);
-            is_member<1>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 1u, blk.y, rq + (2u << hi_shift), best, part);
-            is_member<2>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 2u, blk.z, rq + (1u << hi_shift), best, part);
-            is_member<3>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 3u, blk.w, rq + (3u << hi_shift), best, part);
+            const uint32_t cb = 255u - rq;
+            is_member<ALLG, 0>(n, rv, gr, NG, tilt_mask, mfac, wd, cc, blk.x, cb, best, part);
+            is_member<ALLG, 1>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 1u, blk.y, cb - (2u << hi_shift), best, part);
+            is_member<ALLG, 2>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 2u, blk.z, cb - (1u << hi_shift), best, part);
+            is_member<ALLG, 3>(n, rv, gr, NG, tilt_mask, mfac, wd, cc + 3u, blk.w, cb - (3u << hi_shift), best, part);
         }
         tree_push(i, part, stack, sum);
     }
@@ -451,7 +456,7 @@ static __device__ __forceinline__ bool is_race_coded(const Net &n, uint32_t C, u
     return true;
 }
 
-template <bool SLOTS>
+template <bool SLOTS, bool ALLG>
 __global__ void __launch_bounds__(CSMC_IS_CODED_MAX_THREADS, CSMC_IS_CODED_MIN_CTAS_PER_SM)
     is_coded_kernel(const __grid_constant__ IsParams ip) {
     const SimParams &p = ip.s;
@@ -623,7 +628,7 @@ __global__ void __launch_bounds__(CSMC_IS_CODED_MAX_THREADS, CSMC_IS_CODED_MIN_C
         // ---- the race, the log-likelihood ratio, the winner's transition
         IsBest best;
         double rsum;
-        if (!is_race_coded(n, C, bits, NG, tilt_mask, rv, gr, mfac, p.keys, run, step, best, rsum))
+        if (!is_race_coded<ALLG>(n, C, bits, NG, tilt_mask, rv, gr, mfac, p.keys, run, step, best, rsum))
             is_race_exact(n, C, bits, rv, gr, NG, mfac, p.seed, run, step, best);
         const uint32_t win = bitrev_bits(static_cast<uint32_t>(best.key & 0xffffffffull), bits);
         const float dmin = best.d;
@@ -653,18 +658,18 @@ __global__ void __launch_bounds__(CSMC_IS_CODED_MAX_THREADS, CSMC_IS_CODED_MIN_C
 
 }  // namespace detail
 
-template <bool SLOTS>
+template <bool SLOTS, bool ALLG>
 int is_coded_launch_one(const IsParams &p, int grid, int block, size_t smem, void *stream) {
-    auto fn = detail::is_coded_kernel<SLOTS>;
+    auto fn = detail::is_coded_kernel<SLOTS, ALLG>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     fn<<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return static_cast<int>(cudaGetLastError());
 }
 
-template <bool SLOTS>
+template <bool SLOTS, bool ALLG>
 int is_coded_occupancy_one(int block, size_t smem, int *ctas) {
-    auto fn = detail::is_coded_kernel<SLOTS>;
+    auto fn = detail::is_coded_kernel<SLOTS, ALLG>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
     return static_cast<int>(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, smem));

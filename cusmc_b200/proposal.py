@@ -126,8 +126,9 @@ def set_inference(net, tensor_cores: bool) -> None:
 
 def set_kernel(net, family: int) -> None:
     """Kernel of runs under the proposal: 0 = one thread per run where the
-    network qualifies and the launch has at least 128 runs per SM (else one
-    warp per run), 3 = always one warp per run, 5 = one thread per run
+    network qualifies and the launch has at least 48 runs per SM (128 when a
+    location is outside the tilt groups; else one warp per run), 3 = always
+    one warp per run, 5 = one thread per run
     wherever the network qualifies.  All give the same runs bit for bit."""
     check(lib().csmc_is_set_kernel(net._h, family))
 

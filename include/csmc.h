@@ -276,8 +276,9 @@ int csmc_is_set_inference(csmc_net *net, int32_t tensor_cores);
  * always runs one warp per run).  0 (default): one thread per run (result
  * family 5) when the network has race classes (at most 256 components, 32
  * locations per automaton), theta is evaluated on CUDA cores, the state
- * fits and the launch has at least 128 runs per SM (fewer runs finish
- * sooner one warp per run), else one warp per run (family 3); 3: always one
+ * fits and the launch has at least 48 runs per SM (128 when some location
+ * of the network is outside the tilt groups; fewer runs finish sooner one
+ * warp per run), else one warp per run (family 3); 3: always one
  * warp per run; 5: one thread per run whenever the network qualifies.  The
  * runs, paths and log-likelihood ratios are the same bits either way. */
 int csmc_is_set_kernel(csmc_net *net, int32_t family);

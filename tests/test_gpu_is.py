@@ -147,7 +147,8 @@ def test_theta_cache_keeps_runs_exact_across_launches():
 
 
 def test_launch_size_picks_the_kernel_and_keeps_the_runs():
-    """csmc_is_run's default: one warp per run below 128 runs per SM, one
+    """csmc_is_run's default: one warp per run below 48 runs per SM on a
+    network whose locations are all in tilt groups (the epidemic), one
     thread per run above; the runs they share are the same bits."""
     import torch
     w = netgen.epidemic()
@@ -155,7 +156,7 @@ def test_launch_size_picks_the_kernel_and_keeps_the_runs():
     q = api.variable_query(w.var_id, 100, threshold=49, is_max=True, max_steps=100_000)
     params = _random_proposal(6).pack()
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    big, small = 4 * 32 * sms + 1000, 2000
+    big, small = 48 * sms + 1000, 2000
     net = api.Network(blob)
     P.set_inference(net, False)
     try:
