@@ -194,6 +194,10 @@ _SIGNATURES = {
                                         ctypes.c_void_p]),
     "csmc_mlp_grad": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "csmc_mlp_adam": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.c_void_p]),
     "csmc_mlp_rows_merge": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p]),
     "csmc_ce_select": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,

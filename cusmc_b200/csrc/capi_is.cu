@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -387,6 +389,37 @@ __global__ void reduce_mlp_partials(const float *partials, const double *objecti
     }
 }
 
+// FP32 master vector -> the BF16 parameter block, the host packing's layout
+// (w1 and w2 rounded to BF16, biases and the output layer FP32, padding
+// zero); one thread per entry.
+__global__ void mlp_pack_params(const float *x, csmc::MlpParams *P) {
+    constexpr int H = CSMC_MLP_HID, I = CSMC_MLP_IN;
+    const int k = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k < H * I) (&P->w1[0][0])[k] = csmc::f_to_bf16(x[k]);
+    else if (k < H * I + H) P->b1[k - H * I] = x[k];
+    else if (k < H * I + H + H * H) (&P->w2[0][0])[k - H * I - H] = csmc::f_to_bf16(x[k]);
+    else if (k < H * I + 2 * H + H * H) P->b2[k - H * I - H - H * H] = x[k];
+    else if (k < H * I + 3 * H + H * H) P->w3[k - H * I - 2 * H - H * H] = x[k];
+    else if (k < kGradFloats) P->b3 = x[k];
+    else if (k < kGradFloats + 3) P->pad[k - kGradFloats] = 0.0f;
+}
+
+// One Adam ascent step per entry (csmc_mlp_adam's formulas, every operation
+// an IEEE double operation rounded to nearest, x rounded to FP32).
+__global__ void mlp_adam_ascend(float *x, double *m, double *v, const float *g, double lr, double c1, double c2) {
+    constexpr double b1 = 0.9, b2 = 0.999, eps = 1e-8;
+    const int k = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= kGradFloats) return;
+    const double gi = static_cast<double>(g[k]);
+    const double mk = csmc::d_add(csmc::d_mul(b1, m[k]), csmc::d_mul(1.0 - b1, gi));
+    const double vk = csmc::d_add(csmc::d_mul(b2, v[k]), csmc::d_mul(csmc::d_mul(1.0 - b2, gi), gi));
+    m[k] = mk;
+    v[k] = vk;
+    const double mh = csmc::d_div(mk, c1), vh = csmc::d_div(vk, c2);
+    const double up = csmc::d_div(csmc::d_mul(lr, mh), csmc::d_add(csmc::d_sqrt(vh), eps));
+    x[k] = static_cast<float>(csmc::d_add(static_cast<double>(x[k]), up));
+}
+
 // Device buffers of the proposal-network kernels, one set per device, kept
 // for the life of the process (allocating per call would hand the memory
 // back to the driver at every synchronisation); a call holds the set's lock
@@ -399,6 +432,9 @@ struct MlpDevScratch {
     int *error = nullptr;
     float *grad = nullptr;
     double *J = nullptr;
+    float *x = nullptr;         // Adam: master vector
+    double *moments = nullptr;  // Adam: m, then v
+    double *Js = nullptr;       // Adam: J at the first and the last step
     int grid_cap = 0;
 };
 
@@ -415,6 +451,12 @@ int mlp_scratch_ensure(MlpDevScratch &m, int grid) {
     cudaFree(m.error);
     cudaFree(m.grad);
     cudaFree(m.J);
+    cudaFree(m.x);
+    cudaFree(m.moments);
+    cudaFree(m.Js);
+    m.x = nullptr;
+    m.moments = nullptr;
+    m.Js = nullptr;
     m.P = nullptr;
     m.partials = nullptr;
     m.objective = nullptr;
@@ -429,6 +471,9 @@ int mlp_scratch_ensure(MlpDevScratch &m, int grid) {
     CK(cudaMalloc(&m.error, sizeof(int)), "cudaMalloc(error flag)");
     CK(cudaMalloc(&m.grad, kGradFloats * sizeof(float)), "cudaMalloc(gradient)");
     CK(cudaMalloc(&m.J, sizeof(double)), "cudaMalloc(objective)");
+    CK(cudaMalloc(&m.x, kGradFloats * sizeof(float)), "cudaMalloc(Adam master vector)");
+    CK(cudaMalloc(&m.moments, 2 * kGradFloats * sizeof(double)), "cudaMalloc(Adam moments)");
+    CK(cudaMalloc(&m.Js, 2 * sizeof(double)), "cudaMalloc(Adam objectives)");
     m.grid_cap = grid;
     return CSMC_OK;
 }
@@ -468,9 +513,66 @@ int mlp_common(int mode, const void *params, const void *rows, uint64_t n_rows, 
     return CSMC_OK;
 }
 
+int mlp_adam(const void *rows, uint64_t n_rows, int32_t steps, double lr, float *x, double *mom1, double *mom2,
+             int32_t *t, double *j_first, double *j_last, void *stream) {
+    if (!x || !mom1 || !mom2 || !t || (!rows && n_rows)) return fail(CSMC_ERR_ARG, "null argument");
+    if (steps < 1 || *t < 0 || *t > INT32_MAX - steps) return fail(CSMC_ERR_ARG, "Adam: steps must be positive");
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev), "cudaGetDevice");
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+    const uint64_t tiles = (n_rows + 127) / 128;
+    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, sms)));
+    const int pf = csmc::mlp_tc_partial_floats();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    MlpDevScratch &m = mlp_scratch(dev);
+    std::lock_guard<std::mutex> lock(m.mu);
+    int rc = mlp_scratch_ensure(m, sms);
+    if (rc) return rc;
+    const size_t xb = kGradFloats * sizeof(float), mb = kGradFloats * sizeof(double);
+    CK(cudaMemsetAsync(m.error, 0, sizeof(int), st), "cudaMemsetAsync");
+    CK(cudaMemcpyAsync(m.x, x, xb, cudaMemcpyHostToDevice, st), "upload master vector");
+    CK(cudaMemcpyAsync(m.moments, mom1, mb, cudaMemcpyHostToDevice, st), "upload moments");
+    CK(cudaMemcpyAsync(m.moments + kGradFloats, mom2, mb, cudaMemcpyHostToDevice, st), "upload moments");
+    constexpr int kThreads = 256, kBlocks = (kGradFloats + 3 + kThreads - 1) / kThreads;
+    int32_t tt = *t;
+    for (int32_t s = 0; s < steps; ++s) {
+        mlp_pack_params<<<kBlocks, kThreads, 0, st>>>(m.x, m.P);
+        CK(cudaGetLastError(), "parameter packing launch");
+        rc = csmc::mlp_tc_launch(1, static_cast<const csmc::MlpRow *>(rows), n_rows, m.P, nullptr, m.partials,
+                                 m.objective, m.error, grid, st);
+        if (rc) return cuda_fail(static_cast<cudaError_t>(rc), "tensor-core kernel launch");
+        reduce_mlp_partials<<<(kGradFloats + 255) / 256, 256, 0, st>>>(m.partials, m.objective, grid, pf, m.grad,
+                                                                        m.Js + (s == 0 ? 0 : 1));
+        CK(cudaGetLastError(), "gradient reduction launch");
+        ++tt;
+        const double c1 = 1.0 - std::pow(0.9, static_cast<double>(tt));
+        const double c2 = 1.0 - std::pow(0.999, static_cast<double>(tt));
+        mlp_adam_ascend<<<kBlocks, kThreads, 0, st>>>(m.x, m.moments, m.moments + kGradFloats, m.grad, lr, c1, c2);
+        CK(cudaGetLastError(), "Adam step launch");
+    }
+    int err = 0;
+    double Js[2] = {0.0, 0.0};
+    CK(cudaMemcpyAsync(&err, m.error, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CK(cudaMemcpyAsync(Js, m.Js, sizeof Js, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CK(cudaMemcpyAsync(x, m.x, xb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CK(cudaMemcpyAsync(mom1, m.moments, mb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CK(cudaMemcpyAsync(mom2, m.moments + kGradFloats, mb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CK(cudaStreamSynchronize(st), "Adam steps");
+    if (err) return fail(CSMC_ERR_TIMEOUT, "tensor-core kernel: a bounded wait for the MMA units gave up");
+    *t = tt;
+    if (j_first) *j_first = Js[0];
+    if (j_last) *j_last = steps == 1 ? Js[0] : Js[1];
+    return CSMC_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int csmc_mlp_adam(const void *rows, uint64_t n_rows, int32_t steps, double lr, float *x, double *m, double *v,
+                  int32_t *t, double *j_first, double *j_last, void *stream) {
+    return mlp_adam(rows, n_rows, steps, lr, x, m, v, t, j_first, j_last, stream);
+}
 
 int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, float *theta, void *stream) {
     if (!theta && n_rows) return fail(CSMC_ERR_ARG, "null argument");

@@ -2,14 +2,16 @@
 // ABI, for hosts without Python (the CLI's --csmc-is, C/C++ programs):
 // csmc_is_train runs the whole multi-level CE loop on the GPU — runs under
 // the current proposal (csmc_is_run), elite selection (csmc_ce_select),
-// replay of the elite runs into training rows (csmc_is_trace), Adam ascent
-// on the tensor-core gradient (csmc_mlp_grad) — and returns the trained FP32
-// master parameters and a per-round log.
+// replay of the elite runs into training rows (csmc_is_trace), the row
+// merge (csmc_mlp_rows_merge), Adam ascent on the tensor-core gradient, all
+// steps of a round on the device (csmc_mlp_adam) — and returns the trained
+// FP32 master parameters and a per-round log.
 //
-// The elite selection is host code shared with the Python training loop
-// (cusmc_b200/proposal.py calls csmc_ce_select), so both loops select the
-// same runs from the same values; the loop itself, Adam and the BF16 packing
-// are written independently on both sides, and a GPU test requires the two
+// The elite selection and the Adam steps are library code shared with the
+// Python training loop (cusmc_b200/proposal.py calls csmc_ce_select and
+// csmc_mlp_adam), so both loops select the same runs and take the same
+// steps; the loop itself and the BF16 packing of the runs' parameters are
+// written independently on both sides, and a GPU test requires the two
 // trainings to end with the same parameters bit for bit.
 #include "../../include/csmc.h"
 #include "capi_internal.h"
@@ -134,24 +136,12 @@ void pack(const float *x, csmc::MlpParams &P) {
     P.b3 = x[o++];
 }
 
-// Adam ascent in double precision: m, v moments; x += lr mh / (sqrt(vh) + eps).
-struct Adam {
+// Adam's moments and step count across the rounds (the steps themselves run
+// on the device: csmc_mlp_adam).
+struct AdamState {
     std::vector<double> m, v;
-    int t = 0;
-    double lr, b1 = 0.9, b2 = 0.999, eps = 1e-8;
-    explicit Adam(double lr_) : m(kFloats, 0.0), v(kFloats, 0.0), lr(lr_) {}
-    void ascend(float *x, const float *g) {
-        ++t;
-        const double c1 = 1.0 - std::pow(b1, static_cast<double>(t));
-        const double c2 = 1.0 - std::pow(b2, static_cast<double>(t));
-        for (int i = 0; i < kFloats; ++i) {
-            const double gi = static_cast<double>(g[i]);
-            m[i] = b1 * m[i] + (1.0 - b1) * gi;
-            v[i] = b2 * v[i] + (1.0 - b2) * gi * gi;
-            const double mh = m[i] / c1, vh = v[i] / c2;
-            x[i] = static_cast<float>(static_cast<double>(x[i]) + lr * mh / (std::sqrt(vh) + eps));
-        }
-    }
+    int32_t t = 0;
+    AdamState() : m(kFloats, 0.0), v(kFloats, 0.0) {}
 };
 
 struct DevBuf {
@@ -187,7 +177,7 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
                                   "positive and rho in (0, 1)");
     const uint64_t n = cfg.runs_per_round;
     std::vector<float> x(init, init + kFloats);
-    Adam opt(cfg.lr);
+    AdamState opt;
     DevBuf d_flags, d_logw, d_values, d_steps, d_rows, d_merged, d_elite, d_w, d_off;
     cudaError_t e = d_flags.ensure(n);
     if (e == cudaSuccess) e = d_logw.ensure(n * sizeof(double));
@@ -197,7 +187,6 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
     std::vector<double> h_values(n), h_logw(n);
     std::vector<uint32_t> h_steps(n);
     csmc::MlpParams P;
-    std::vector<float> g(kFloats);
     int at_goal = 0, done = 0;
     for (int32_t k = 0; k < cfg.rounds; ++k) {
         const auto t0 = std::chrono::steady_clock::now();
@@ -236,13 +225,9 @@ int train(csmc_net *net, const csmc_query *q, uint64_t seed, const csmc_ce_confi
         const double trace_s = seconds_since(t1);
         const auto t2 = std::chrono::steady_clock::now();
         double J0 = 0.0, J = 0.0;
-        for (int32_t st = 0; st < cfg.adam_steps; ++st) {
-            pack(x.data(), P);
-            rc = csmc_mlp_grad(&P, d_merged.p, m_rows, g.data(), &J, nullptr);
-            if (rc) return rc;
-            if (st == 0) J0 = J;
-            opt.ascend(x.data(), g.data());
-        }
+        rc = csmc_mlp_adam(d_merged.p, m_rows, cfg.adam_steps, cfg.lr, x.data(), opt.m.data(), opt.v.data(), &opt.t,
+                           &J0, &J, nullptr);
+        if (rc) return rc;
         const double adam_s = seconds_since(t2);
         if (log && k < log_cap) {
             csmc_ce_round &L = log[k];

@@ -14,7 +14,8 @@ values), weights each elite run by its likelihood ratio, replays the elite
 runs on the GPU into training rows (four per step: features, a, b), and
 takes Adam steps on J = sum (b theta - a e^theta), the weighted
 log-likelihood of the elite paths under the proposal up to a constant; the
-gradient of J comes from the tensor-core kernel (csmc_mlp_grad).
+gradient of J comes from the tensor-core kernel, and a round's Adam steps
+run on the device (csmc_mlp_adam).
 """
 from __future__ import annotations
 
@@ -96,21 +97,27 @@ class Proposal:
         return bytes(out)
 
 
-class Adam:
-    def __init__(self, n: int, lr: float = 1e-2, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+class AdamState:
+    """Adam's moments and step count across CE rounds (the steps run on the
+    device: adam_run)."""
+
+    def __init__(self, n: int = GRAD_FLOATS):
         self.m = np.zeros(n, np.float64)
         self.v = np.zeros(n, np.float64)
         self.t = 0
-        self.lr, self.b1, self.b2, self.eps = lr, b1, b2, eps
 
-    def ascend(self, x: np.ndarray, g: np.ndarray) -> np.ndarray:
-        self.t += 1
-        g = np.asarray(g, np.float64)
-        self.m = self.b1 * self.m + (1 - self.b1) * g
-        self.v = self.b2 * self.v + (1 - self.b2) * g * g
-        mh = self.m / (1 - self.b1 ** self.t)
-        vh = self.v / (1 - self.b2 ** self.t)
-        return (x + self.lr * mh / (np.sqrt(vh) + self.eps)).astype(np.float32)
+
+def adam_run(rows, n_rows: int, steps: int, lr: float, x: np.ndarray, state: AdamState, stream=None):
+    """csmc_mlp_adam: `steps` Adam ascent steps on J over n_rows device rows
+    (a torch CUDA tensor), on the device; x (FP32 master vector) and state
+    are updated in place.  Returns J at the first and the last step."""
+    assert x.dtype == np.float32 and x.size == GRAD_FLOATS and x.flags.c_contiguous
+    t = ctypes.c_int32(state.t)
+    j0, j1 = ctypes.c_double(), ctypes.c_double()
+    check(lib().csmc_mlp_adam(_ptr(rows), n_rows, steps, lr, x.ctypes.data, state.m.ctypes.data,
+                              state.v.ctypes.data, ctypes.byref(t), ctypes.byref(j0), ctypes.byref(j1), stream))
+    state.t = t.value
+    return j0.value, j1.value
 
 
 def _ptr(t) -> int | None:
@@ -306,7 +313,7 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
     dev = torch.device("cuda")
     prop = Proposal.init(init_seed)
     x = prop.vector()
-    opt = Adam(x.size, lr=lr)
+    opt = AdamState(x.size)
     log = TrainLog()
     n = runs_per_round
     flags = torch.empty(n, dtype=torch.uint8, device=dev)
@@ -333,13 +340,9 @@ def train(net, query: Query, seed: int = 1, rounds: int = 10, runs_per_round: in
         m_rows = merge_rows(rows, t_off, len(elite), n_rows, merged)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-        J0 = None
-        for _ in range(adam_steps):
-            g, J = mlp_grad(prop.pack(), merged, m_rows)
-            if J0 is None:
-                J0 = J
-            x = opt.ascend(x, g)
-            prop = Proposal.from_vector(x)
+        x = np.array(x, dtype=np.float32, copy=True)
+        J0, J = adam_run(merged, m_rows, adam_steps, lr, x, opt)
+        prop = Proposal.from_vector(x)
         t3 = time.perf_counter()
         hit_est = float(res.estimate)
         entry = {"round": k, "level": sel.level, "elite": int(len(elite)), "rows": n_rows, "merged_rows": m_rows,

@@ -327,6 +327,20 @@ int csmc_mlp_forward(const void *params, const void *rows, uint64_t n_rows, floa
 int csmc_mlp_grad(const void *params, const void *rows, uint64_t n_rows, float *grad, double *objective,
                   void *stream);
 
+/* `steps` Adam ascent steps on J over n_rows device rows, on the device with
+ * one synchronisation at the end.  x (the FP32 master vector in the
+ * gradient's layout), m and v (the moments) are host arrays of
+ * CSMC_MLP_GRAD_FLOATS entries and *t the step count, all updated in place.
+ * Each step packs x into the BF16 parameter block, takes csmc_mlp_grad's
+ * gradient g and applies, in IEEE double rounded to nearest, t += 1,
+ * m = 0.9 m + 0.1 g, v = 0.999 v + 0.001 g g (the coefficients as
+ * 1 - 0.9 and 1 - 0.999 in double), x += lr (m / c1) / (sqrt(v / c2) +
+ * 1e-8) with c1 = 1 - 0.9^t and c2 = 1 - 0.999^t from the host's pow,
+ * x rounded to FP32.  *j_first and *j_last: J at the first and the last
+ * step's parameters (before their update). */
+int csmc_mlp_adam(const void *rows, uint64_t n_rows, int32_t steps, double lr, float *x, double *m, double *v,
+                  int32_t *t, double *j_first, double *j_last, void *stream);
+
 /* Merges replayed training rows (device buffers): rows of one listed run and
  * one location class (rows row_offset[i] + l, + 4, ..., up to the next
  * run's first row or n_rows) whose features are equal on consecutive steps

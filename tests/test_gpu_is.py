@@ -359,10 +359,11 @@ def test_ce_training_lowers_the_error_of_a_rare_event_estimate():
 
 def test_c_abi_training_equals_the_python_training():
     """csmc_is_train (the CE loop in the library, for hosts without Python)
-    and proposal.train (the loop in Python: its own Adam in numpy, its own
-    BF16 packing) end with the same parameters bit for bit from the same
+    and proposal.train (the loop in Python, its own BF16 packing of the
+    runs' parameters) end with the same parameters bit for bit from the same
     initial parameters, and log the same rounds.  Both use the library's
-    elite selection (csmc_ce_select) and the same kernels."""
+    elite selection (csmc_ce_select), Adam steps (csmc_mlp_adam) and
+    kernels."""
     w = netgen.epidemic()
     net = api.Network(_blob(w))
     try:
@@ -379,6 +380,56 @@ def test_c_abi_training_equals_the_python_training():
         assert a["J_start"] == b["j_start"] and a["J_end"] == b["j_end"] and a["hits"] == b["hits"]
     assert prop_c.pack() == P.Proposal.from_vector(prop_c.vector()).pack()
 
+
+
+def _host_adam(x, g, m, v, t, lr):
+    """Adam's ascent step in numpy double (csmc_mlp_adam's formulas)."""
+    t += 1
+    g = np.asarray(g, np.float64)
+    m = 0.9 * m + (1 - 0.9) * g
+    v = 0.999 * v + (1 - 0.999) * g * g
+    mh = m / (1 - 0.9 ** t)
+    vh = v / (1 - 0.999 ** t)
+    return (x + lr * mh / (np.sqrt(vh) + 1e-8)).astype(np.float32), m, v, t
+
+
+def test_device_adam_equals_the_host_steps():
+    """csmc_mlp_adam (a round's Adam steps on the device, one
+    synchronisation) against the same steps on the host: csmc_mlp_grad at
+    the host-packed parameters, then Adam's update in numpy double.  The
+    master vector, both moments, the step count and the first and last
+    objectives of each call are equal bit for bit over two calls (the
+    moments carry from one call to the next)."""
+    import torch
+    n = 50_000
+    rng = np.random.default_rng(11)
+    x = np.zeros((n, P.IN), np.float32)
+    x[np.arange(n), rng.integers(0, 4, n)] = 1.0
+    x[:, 5:9] = rng.dirichlet([4, 1, 1, 4], n).astype(np.float32)
+    x[:, 9] = rng.uniform(0, 1, n)
+    rows = np.zeros(n, dtype=np.dtype([("x", "<u2", (P.IN,)), ("a", "<f4"), ("b", "<f4")]))
+    rows["x"] = P.f32_to_bf16_bits(x.ravel()).reshape(n, P.IN)
+    rows["a"] = rng.exponential(1e-3, n).astype(np.float32)
+    rows["b"] = (rng.uniform(0, 1, n) < 0.3).astype(np.float32) * rng.uniform(0.5, 2.0, n).astype(np.float32)
+    dev_rows = torch.from_numpy(rows.view(np.uint8).copy()).cuda()
+    lr = 3e-2
+    x0 = P.Proposal.init(3).vector()
+    xd = x0.copy()
+    state = P.AdamState()
+    ja = P.adam_run(dev_rows, n, 5, lr, xd, state)
+    jb = P.adam_run(dev_rows, n, 3, lr, xd, state)
+    xh, m, v, t = x0.copy(), np.zeros(P.GRAD_FLOATS), np.zeros(P.GRAD_FLOATS), 0
+    Js = []
+    for _ in range(8):
+        g, J = P.mlp_grad(P.Proposal.from_vector(xh).pack(), dev_rows, n)
+        Js.append(J)
+        xh, m, v, t = _host_adam(xh, g, m, v, t, lr)
+    assert state.t == t == 8
+    assert np.array_equal(xd.view(np.uint32), xh.view(np.uint32))
+    assert np.array_equal(state.m.view(np.uint64), m.view(np.uint64))
+    assert np.array_equal(state.v.view(np.uint64), v.view(np.uint64))
+    assert ja == (Js[0], Js[4]) and jb == (Js[5], Js[7])
+    assert not np.array_equal(x0, xh)
 
 
 @pytest.mark.parametrize("case", ["epidemic_permuted", "mutex_clock"])
