@@ -256,6 +256,39 @@ def test_row_merge_keeps_the_objective_and_gradient():
     assert np.linalg.norm(g1 - g0) <= 1e-3 * np.linalg.norm(g0)
 
 
+def test_row_merge_across_batch_boundaries():
+    """Synthetic rows: per chain, features that keep their value from one
+    step to the next with probability 0.9 (groups longer than the merge's
+    32-step batches, and groups that straddle them), chains of 0 to 200
+    steps, a and b zero, negative zero or positive; the GPU merge equals
+    the restated merge byte for byte."""
+    import torch
+    rng = np.random.default_rng(5)
+    lens = [0, 1, 31, 32, 33, 64, 65, 200, 7, 0, 96, 150, 0]
+    offs = np.concatenate([[0], np.cumsum(4 * np.array(lens))[:-1]]).astype(np.uint64)
+    n = 4 * sum(lens)
+    rows = np.zeros(n, dtype=oracle.ROW_DTYPE)
+    feats = rng.integers(0, 2**16, (3, 16)).astype(np.uint16)
+    for b, steps in zip(offs.astype(np.int64), lens):
+        for l in range(4):
+            cur = int(rng.integers(0, 3))
+            for k in range(steps):
+                if rng.uniform() > 0.9:
+                    cur = int(rng.integers(0, 3))
+                rows["x"][b + 4 * k + l] = feats[cur]
+    kind = rng.integers(0, 4, (n, 2))
+    vals = rng.exponential(1.0, (n, 2)).astype(np.float32)
+    ab = np.where(kind == 0, np.float32(-0.0), np.where(kind == 1, np.float32(0.0), vals))
+    rows["a"], rows["b"] = ab[:, 0], ab[:, 1]
+    dev = torch.device("cuda")
+    t_rows = torch.from_numpy(rows.view(np.uint8).copy()).to(dev)
+    merged = torch.zeros_like(t_rows)
+    got_n = P.merge_rows(t_rows, torch.from_numpy(offs.view(np.int64)).to(dev), len(lens), n, merged)
+    ref = _merge_rows_reference(rows, [int(o) for o in offs])
+    assert got_n == len(ref)
+    assert merged.cpu().numpy()[: got_n * P.ROW_BYTES].tobytes() == ref.tobytes()
+
+
 def test_tensor_core_inference_follows_the_exact_paths():
     import torch
     w = netgen.epidemic()
