@@ -50,6 +50,26 @@ def test_upload_without_a_device_fails_loudly(tmp_path):
     assert e.value.code == _native.CSMC_ERR_NODEVICE
 
 
+def test_adam_entry_point_checks_its_arguments_first():
+    """csmc_mlp_adam refuses a missing master vector or moment array and a
+    step count below one before it touches a device."""
+    import numpy as np
+    from cusmc_b200 import proposal as P
+    lib = _native.lib()
+    x = np.zeros(P.GRAD_FLOATS, np.float32)
+    m = np.zeros(P.GRAD_FLOATS, np.float64)
+    v = np.zeros(P.GRAD_FLOATS, np.float64)
+    t = ctypes.c_int32(0)
+    j0, j1 = ctypes.c_double(), ctypes.c_double()
+    assert lib.csmc_mlp_adam(None, 0, 0, 1e-2, x.ctypes.data, m.ctypes.data, v.ctypes.data, ctypes.byref(t),
+                             ctypes.byref(j0), ctypes.byref(j1), None) == _native.CSMC_ERR_ARG
+    assert lib.csmc_mlp_adam(None, 0, 3, 1e-2, None, m.ctypes.data, v.ctypes.data, ctypes.byref(t),
+                             ctypes.byref(j0), ctypes.byref(j1), None) == _native.CSMC_ERR_ARG
+    assert lib.csmc_mlp_adam(None, 5, 3, 1e-2, x.ctypes.data, m.ctypes.data, v.ctypes.data, ctypes.byref(t),
+                             ctypes.byref(j0), ctypes.byref(j1), None) == _native.CSMC_ERR_ARG
+    assert t.value == 0
+
+
 def _cli(*args, cwd=None):
     return subprocess.run([CLI, *args], capture_output=True, text=True, cwd=cwd, timeout=60)
 
