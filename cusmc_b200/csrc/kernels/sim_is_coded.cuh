@@ -41,14 +41,15 @@
 #include "sim_coded.cuh"
 #include "sim_is.cuh"
 
-// Up to 128 threads per CTA.  192-thread CTAs (two per SM, twelve warps)
-// measured slower on the epidemic (561k against 577k-591k runs/s at 1e5
-// runs).
+// Up to 384 threads per CTA, at most 168 registers a thread (384 x 168
+// fills the register file).  A 384-thread CTA keeps one copy of the
+// network and the proposal for twelve warps (one CTA per SM); 128-thread
+// CTAs fit two per SM (eight warps) within shared memory.
 #ifndef CSMC_IS_CODED_MAX_THREADS
-#define CSMC_IS_CODED_MAX_THREADS 128
+#define CSMC_IS_CODED_MAX_THREADS 384
 #endif
 #ifndef CSMC_IS_CODED_MIN_CTAS_PER_SM
-#define CSMC_IS_CODED_MIN_CTAS_PER_SM 3
+#define CSMC_IS_CODED_MIN_CTAS_PER_SM 1
 #endif
 
 namespace csmc {

@@ -149,29 +149,34 @@ def test_theta_cache_keeps_runs_exact_across_launches():
 def test_launch_size_picks_the_kernel_and_keeps_the_runs():
     """csmc_is_run's default: one warp per run below 48 runs per SM on a
     network whose locations are all in tilt groups (the epidemic), one
-    thread per run above; the runs they share are the same bits."""
+    thread per run above, in CTAs of 128 threads and, from 576 runs per SM,
+    of 384; the runs they share are the same bits."""
     import torch
     w = netgen.epidemic()
     blob = _blob(w)
     q = api.variable_query(w.var_id, 100, threshold=49, is_max=True, max_steps=100_000)
     params = _random_proposal(6).pack()
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    big, small = 48 * sms + 1000, 2000
+    huge, big, small = 576 * sms + 1000, 48 * sms + 1000, 2000
     net = api.Network(blob)
     P.set_inference(net, False)
     try:
         dev = torch.device("cuda")
         out = {}
-        for n in (big, small):
+        for n in (huge, big, small):
             logw = torch.zeros(n, dtype=torch.float64, device=dev)
             steps = torch.zeros(n, dtype=torch.int32, device=dev)
             r = P.is_run(net, q, params, 31, n, 100, logw=logw, steps=steps)
-            out[n] = (r.family, logw.cpu().numpy(), steps.cpu().numpy())
+            out[n] = (r.family, logw.cpu().numpy(), steps.cpu().numpy(), r.runs_per_cta)
     finally:
         net.close()
-    assert out[big][0] == 5 and out[small][0] == 3
-    assert np.array_equal(out[big][1][:small].view(np.uint64), out[small][1].view(np.uint64))
-    assert np.array_equal(out[big][2][:small], out[small][2])
+    assert out[huge][0] == 5 and out[huge][3] == 384
+    assert out[big][0] == 5 and out[big][3] in (32, 64, 128)
+    assert out[small][0] == 3
+    for n in (huge, big):
+        assert np.array_equal(out[n][1][:small].view(np.uint64), out[small][1].view(np.uint64))
+        assert np.array_equal(out[n][2][:small], out[small][2])
+    assert np.array_equal(out[huge][1][:big].view(np.uint64), out[big][1].view(np.uint64))
 
 
 def test_replay_rows_match_the_oracle():
